@@ -1,0 +1,281 @@
+#!/usr/bin/env python3
+"""Benchmark of the COTHER search path on B200.
+
+One step = one query profile searched against the GPU-resident synthetic
+database through the whole implemented pipeline. Metric: GCUPS = query
+length x database positions / time.
+
+  value  -- GCUPS from the device time of the pipeline's kernels (inputs
+            already resident in HBM);
+  e2e    -- GCUPS of the C-ABI call a user makes (cbp_process): host query
+            buffers are packed and copied to the device and the results are
+            read back inside the timed region.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: launched by torchrun, one rank per GPU; every rank searches its
+own database shard of the full configured size (weak scaling), no
+collective on the data path; the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DEFAULT_WORKLOAD = "q400_db50k"
+OPS_PER_DDMS_STEP = 50  # algorithmic ops of one 4-cell DDMS step (2 pair scores,
+                        # 2 interpolations, 4 segment updates, 1 top-3 register)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
+    ap.add_argument("--ndb", type=int, default=None, help="override #database profiles (testing only)")
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def ddms_steps(L1: int, L2: int, dstsegm: int = 6) -> int:
+    """Exact number of 4-cell DDMS steps for lists of lengths L1, L2."""
+    if L1 < dstsegm or L2 < dstsegm:
+        return 0
+    n = 0
+    j = L2 >> 2
+    while j >= 0:
+        lim = min(L1, L2 - j)
+        n += (lim + 3) // 4 if lim > 0 else 0
+        j -= 2
+    i = L1 >> 2
+    while i > 0:
+        lim = min(L2, L1 - i)
+        n += (lim + 3) // 4 if lim > 0 else 0
+        i -= 2
+    return n
+
+
+def total_ddms_steps(q, db) -> int:
+    hq = np.bincount(q.dd[0].astype(np.int64), minlength=100)
+    hd = np.bincount(db.dd[0].astype(np.int64), minlength=100)
+    tab = np.array([[ddms_steps(a, b) for b in range(100)] for a in range(100)], np.int64)
+    return int(hq @ tab @ hd)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if p[5 + k].lower() in ("active", "1"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def cpu_baseline(q, db, ss, seconds: float):
+    """Oracle (a port of the reference kernels) on the host cores, on a
+    bounded sample: the query against the first database profiles."""
+    from oracle import oracle as O
+    ncpu = os.cpu_count() or 1
+    # calibrate on a small sample, then size the timed sample
+    probe = int(min(db.npositions, 64))
+    t = time.perf_counter()
+    O.score_matrix(q, db, ss, ncols=probe, nthreads=ncpu)
+    dt = max(time.perf_counter() - t, 1e-3)
+    rate = q.npositions * probe / dt
+    ncols = int(min(db.npositions, max(probe, rate * seconds / q.npositions)))
+    t = time.perf_counter()
+    O.score_matrix(q, db, ss, ncols=ncols, nthreads=ncpu)
+    dt = time.perf_counter() - t
+    cells = q.npositions * ncols
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": ncpu, "kind": "port",
+            "sample": f"query {q.npositions} x first {ncols} database positions "
+                      f"({cells} cells, {dt:.1f} s), score-matrix stage"}
+
+
+def run_reference(args):
+    """--impl reference: the oracle port of the reference's kernels on the
+    host cores (the reference has no CPU path of its own)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from cother_b200 import synth
+    ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
+    ndb = args.ndb or 200
+    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=ndb)
+    vals = []
+    for _ in range(max(1, args.warmup) + args.steps):
+        vals.append(cpu_baseline(q, db, ss, args.cpu_seconds / 3))
+    timed = vals[-args.steps:] if args.steps > 0 else vals
+    v = float(np.mean([x["value"] for x in timed]))
+    cb = dict(timed[-1])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "stages": ["score_matrix"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    import cother_b200 as cb
+    from cother_b200 import synth
+    ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
+    q, db = synth.make_workload(args.workload, seed=args.seed + 1000 * rank, ndb=args.ndb)
+    Lq, Ndb = q.npositions, db.npositions
+    steps_ddms = total_ddms_steps(q, db)
+
+    bp = cb.BatchProcessing(ss, device=local)
+    bp.transfer_cpm_data(db)
+    bp.set_db_details(Ndb * world, db.nprofiles * world)
+    bp.set_query_len(Lq)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        bp.process_score_matrix(q)
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    kern_ms, launches = 0.0, 0
+    score_ms = 0.0
+    e0.record(stream)
+    for _ in range(args.steps):
+        bp.process_score_matrix(q)
+        st = bp.stage_times()
+        kern_ms += sum(st)
+        score_ms += st[0]
+        launches += bp.launch_count()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    clocks = clk.stop()
+    t = torch.tensor([e2e_ms, kern_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms, kern_ms = float(t[0]), float(t[1])
+    cells = float(Lq) * float(Ndb) * world
+    steps = max(args.steps, 1)
+    value = cells * steps / (kern_ms / 1e3) / 1e9
+    e2e = cells * steps / (e2e_ms / 1e3) / 1e9
+
+    if rank == 0:
+        peaks = measured_peaks()
+        score_launch_ms = score_ms / max(1, launches)
+        ops = steps_ddms * OPS_PER_DDMS_STEP * world / world  # per rank, per launch
+        achieved = ops / (score_launch_ms / 1e3) / 1e9  # Gop/s
+        sm_mhz = clocks.get("sm_max_mhz") or 1965.0
+        alu_peak = 148 * 128 * sm_mhz * 1e6 / 1e9  # lane-ops/s at max clock, Gop/s
+        roof = {"bound": "alu", "achieved": achieved, "peak": alu_peak, "unit": "Gop/s",
+                "frac": achieved / alu_peak, "traffic": None,
+                "kernel": "score_matrix_kernel",
+                "peak_source": "148 SMs x 128 FP32 lanes x max SM clock (nominal issue rate)",
+                "hbm_bytes_per_launch": float(Lq) * Ndb * 8,
+                "hbm_peak_gbs": (peaks or {}).get("hbm_gbs")}
+        line = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern_ms / steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": args.workload, "query_len": Lq, "db_profiles": db.nprofiles,
+                           "db_positions": Ndb, "stages": ["score_matrix"],
+                           "l2": "inputs larger than L2 (database chunk > 126 MB)",
+                           "parallelism": f"dp{world} (database shard per GPU)"},
+                "e2e": {"value": e2e, "unit": "GCUPS",
+                        "h2d_bytes_per_step": int(Lq * (4 * 20 + 4 * 3 + 4 * 100 + 2) + 4 * 7 * (Lq + 1)),
+                        "d2h_bytes_per_step": 0},
+                "gpu_launches": launches, "roofline": roof, "clocks": clocks}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds)
+        print(json.dumps(line))
+    bp.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,183 @@
+"""cother_b200 -- B200-native search path of COTHER.
+
+The search path (score matrix, phase-1 DP, statistics, MAP realignment,
+hit records) runs in ``libcother_b200.so``: hand-written sm_100a CUDA
+kernels behind the C ABI declared in ``include/cother_b200.h``. This module
+binds that ABI with ctypes and mirrors the reference's per-worker driver
+interface (``CuBatchProcessing``, src/libmycu/cupro/CuBatchProcessing.cuh:47-244)
+as :class:`BatchProcessing`.
+
+There is no CPU fallback: if the library cannot be loaded, or no GPU is
+present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+__all__ = ["Options", "BatchProcessing", "CbpError", "load_library", "LIB_PATH"]
+
+LIB_PATH = _build.LIB_MAIN
+
+_lib = None
+
+
+class CbpError(RuntimeError):
+    """A failure reported by the native library (status code + message)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Options(ctypes.Structure):
+    """Path options (``cbp_options``; MOptions of the reference)."""
+
+    _fields_ = [
+        ("ssswgt", ctypes.c_float), ("cvswgt", ctypes.c_float), ("ddmswgt", ctypes.c_float),
+        ("dstsegm", ctypes.c_int), ("mapaln", ctypes.c_int), ("minpp", ctypes.c_float),
+        ("ssemodel", ctypes.c_int), ("x_uninf", ctypes.c_int), ("eval", ctypes.c_float),
+        ("nohits", ctypes.c_int), ("noalns", ctypes.c_int),
+    ]
+
+    @classmethod
+    def defaults(cls) -> "Options":
+        o = cls()
+        load_library().cbp_default_options(ctypes.byref(o))
+        return o
+
+
+def load_library(path: str | None = None):
+    """Load (and bind) the native library; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise CbpError(-1, f"native library not built: {path} (run __graft_entry__.build())")
+    L = ctypes.CDLL(path)
+    vp, sz, i32, f32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_float
+    sig = {
+        "cbp_default_options": (None, [vp]),
+        "cbp_last_error": (ctypes.c_char_p, []),
+        "cbp_create": (i32, [i32, vp, vp, sz, ctypes.POINTER(vp)]),
+        "cbp_destroy": (i32, [vp]),
+        "cbp_set_db_details": (i32, [vp, ctypes.c_uint64, sz]),
+        "cbp_set_query_len": (i32, [vp, sz]),
+        "cbp_set_score_threshold": (i32, [vp, f32]),
+        "cbp_set_logE_threshold": (i32, [vp, f32]),
+        "cbp_transfer_chunk": (i32, [vp, vp, vp, vp]),
+        "cbp_process": (i32, [vp, i32, sz, vp, vp]),
+        "cbp_wait_idle": (i32, [vp]),
+        "cbp_read_score_matrix": (i32, [vp, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
+        "cbp_set_max_slab_positions": (i32, [vp, sz]),
+        "cbp_stage_times": (i32, [vp, vp, i32]),
+        "cbp_launch_count": (i32, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        msg = load_library().cbp_last_error()
+        raise CbpError(rc, msg.decode() if msg else "")
+
+
+class BatchProcessing:
+    """One search context on one GPU (the reference's CuBatchProcessing).
+
+    Method names follow the reference's (TransferCPMData, SetDbDetails,
+    ProcessScoreMatrix ...) in Python style.
+    """
+
+    def __init__(self, ss_table: np.ndarray, options: Options | None = None, device: int = 0,
+                 dev_mem_bytes: int = 0):
+        L = load_library()
+        self._opt = options or Options.defaults()
+        self._ss = np.ascontiguousarray(ss_table, dtype=np.float32)
+        if self._ss.shape != (30, 30):
+            raise ValueError("ss_table must be 30x30")
+        h = ctypes.c_void_p()
+        _check(L.cbp_create(device, ctypes.byref(self._opt), self._ss.ctypes.data, dev_mem_bytes,
+                            ctypes.byref(h)))
+        self._h = h
+        self._db = None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load_library().cbp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- settings (CuBatchProcessing::Set*) ---
+    def set_db_details(self, db_len: int, n_seqs: int) -> None:
+        _check(load_library().cbp_set_db_details(self._h, int(db_len), int(n_seqs)))
+
+    def set_query_len(self, qlen: int) -> None:
+        _check(load_library().cbp_set_query_len(self._h, int(qlen)))
+
+    def set_score_threshold(self, t: float) -> None:
+        _check(load_library().cbp_set_score_threshold(self._h, float(t)))
+
+    def set_logE_threshold(self, t: float) -> None:
+        _check(load_library().cbp_set_logE_threshold(self._h, float(t)))
+
+    def set_max_slab_positions(self, n: int) -> None:
+        _check(load_library().cbp_set_max_slab_positions(self._h, int(n)))
+
+    # --- data and processing ---
+    def transfer_cpm_data(self, db) -> None:
+        """Upload a database chunk (a ProfileSet) and keep it resident."""
+        beg, end = db.field_tables()
+        _check(load_library().cbp_transfer_chunk(self._h, beg, end, None))
+        self._db = db
+
+    def process_score_matrix(self, query, query_serial: int = 0) -> None:
+        """Search one query profile against the resident chunk."""
+        beg, end = query.field_tables()
+        _check(load_library().cbp_process(self._h, int(query_serial), int(query.npositions), beg, end))
+
+    def wait_idle(self) -> None:
+        _check(load_library().cbp_wait_idle(self._h))
+
+    # --- inspection ---
+    def read_score_matrix(self, nrows: int, max_cols: int):
+        """(scores, modscores, first_profile) of the last processed slab."""
+        sc = np.zeros((nrows, max_cols), np.float32)
+        ms = np.zeros((nrows, max_cols), np.float32)
+        ncols = ctypes.c_size_t()
+        first = ctypes.c_size_t()
+        _check(load_library().cbp_read_score_matrix(self._h, sc.ctypes.data, ms.ctypes.data, max_cols,
+                                                     ctypes.byref(ncols), ctypes.byref(first)))
+        n = ncols.value
+        return sc[:, :n], ms[:, :n], first.value
+
+    def stage_times(self) -> list:
+        buf = (ctypes.c_float * 6)()
+        n = load_library().cbp_stage_times(self._h, buf, 6)
+        return [buf[i] for i in range(n)]
+
+    def launch_count(self) -> int:
+        v = ctypes.c_uint64()
+        _check(load_library().cbp_launch_count(self._h, ctypes.byref(v)))
+        return int(v.value)

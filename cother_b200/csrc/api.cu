@@ -1,0 +1,486 @@
+// C ABI and host driver of the search path (the role of the reference's
+// CuBatchProcessing, src/libmycu/cupro/CuBatchProcessing.cu:189-697, and of
+// its device-memory planner CuDeviceMemory, src/libmycu/cupro/CuDeviceMemory.cu).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "cother_b200.h"
+#include "common.cuh"
+#include "layout.h"
+#include "score_kernel.cuh"
+
+namespace cbp {
+
+// field indices (src/libmycu/cupro/PM2DVectorFields.h:51-87)
+enum {
+    fBkg = 0, fENO = 20, fLen = 21, fDist = 22, fTrn = 23, fTF = 30, fCV = 50,
+    fDD = 71, fSS = 171, fAddrPro = 176, fAA = 179, fSSstate = 180, fTot = 181
+};
+
+static thread_local std::string g_last_error;
+
+// A device buffer that only grows.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t n) {
+        if (n <= bytes) return;
+        if (p) CBP_CUDA(cudaFree(p));
+        p = nullptr; bytes = 0;
+        CBP_CUDA(cudaMalloc(&p, n));
+        bytes = n;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr; bytes = 0;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Device copy of a packed profile set.
+struct ProfilesStore {
+    DevBuf tf, ss, dst, dstlen, trn, bkg, eno, plen, pstart, pro, aa, sss;
+    ProfilesDev view;
+    std::vector<int> h_plen;
+    std::vector<long long> h_pstart;
+    void release() {
+        for (DevBuf* b : {&tf, &ss, &dst, &dstlen, &trn, &bkg, &eno, &plen, &pstart, &pro, &aa, &sss})
+            b->release();
+        view = ProfilesDev();
+        h_plen.clear();
+        h_pstart.clear();
+    }
+};
+
+}  // namespace cbp
+
+using namespace cbp;
+
+struct cbp_context {
+    int device = 0;
+    cbp_options opt{};
+    cudaStream_t stream = nullptr;
+    float sstab_h[kSSCard * kSSCard];
+    float dmstab_h[kDstCard * kDstCard];
+    DevBuf sstab, dmstab;
+    ProfilesStore db, query;
+    bool have_db = false;
+    size_t mem_budget = 0;
+    size_t max_slab_positions = 0;
+    // settings
+    uint64_t db_len = 0;
+    size_t n_seqs = 0;
+    size_t query_len = 0;
+    float score_thld = 0.f;
+    float logE_thld = 0.f;
+    // working buffers
+    DevBuf scores, modscores;
+    // last slab
+    long long last_col0 = 0;
+    int last_ncols = 0;
+    long long last_ld = 0;
+    int last_first_profile = 0;
+    int last_Lq = 0;
+    // instrumentation
+    cudaEvent_t ev[8]{};
+    float stage_ms[6] = {0, 0, 0, 0, 0, 0};
+    uint64_t launches = 0;
+};
+
+namespace {
+
+template <class F>
+int guarded(F&& f)
+{
+    try {
+        f();
+        g_last_error.clear();
+        return CBP_OK;
+    } catch (const cbp::Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return CBP_ERR_ARG;
+    }
+}
+
+void parallel_for(long long n, const std::function<void(long long, long long)>& fn)
+{
+    int nt = (int)std::min<long long>(std::max(1u, std::thread::hardware_concurrency()), 32);
+    if (n < 65536 || nt <= 1) { fn(0, n); return; }
+    std::vector<std::thread> th;
+    long long per = (n + nt - 1) / nt;
+    for (int t = 0; t < nt; t++) {
+        long long a = t * per, b = std::min(n, a + per);
+        if (a >= b) break;
+        th.emplace_back(fn, a, b);
+    }
+    for (auto& x : th) x.join();
+}
+
+size_t field_bytes(char* const* beg, char* const* end, int f)
+{
+    if (!beg[f] || !end[f] || end[f] < beg[f])
+        throw Error(CBP_ERR_ARG, "field " + std::to_string(f) + ": invalid begin/end pointers");
+    return (size_t)(end[f] - beg[f]);
+}
+
+// Repack 181 SoA host fields into the device layout (layout.h) and upload.
+void upload_profiles(ProfilesStore& st, char* const* beg, char* const* end, cudaStream_t stream)
+{
+    if (!beg || !end) throw Error(CBP_ERR_ARG, "null field tables");
+    const size_t P = field_bytes(beg, end, fLen) / sizeof(int);
+    const size_t N = field_bytes(beg, end, fTF) / sizeof(float);
+    if (P == 0 || N == 0) throw Error(CBP_ERR_ARG, "empty profile set");
+    if (field_bytes(beg, end, fTrn) / sizeof(float) != N + P)
+        throw Error(CBP_ERR_ARG, "transition fields must hold N+P entries");
+    for (int a = 0; a < kNAA; a++) {
+        if (field_bytes(beg, end, fTF + a) != N * sizeof(float))
+            throw Error(CBP_ERR_ARG, "target-frequency fields of unequal size");
+        if (field_bytes(beg, end, fBkg + a) != P * sizeof(float))
+            throw Error(CBP_ERR_ARG, "background fields of unequal size");
+    }
+    for (int s = 0; s < 100; s++)
+        if (field_bytes(beg, end, fDD + s) != N * sizeof(float))
+            throw Error(CBP_ERR_ARG, "distance fields of unequal size");
+    const int* lens = reinterpret_cast<const int*>(beg[fLen]);
+    const uint32_t* dists = reinterpret_cast<const uint32_t*>(beg[fDist]);
+    st.h_plen.assign(lens, lens + P);
+    st.h_pstart.resize(P);
+    long long acc = 0;
+    for (size_t p = 0; p < P; p++) {
+        if (lens[p] <= 0) throw Error(CBP_ERR_ARG, "profile of non-positive length");
+        if (lens[p] >= 65536) throw Error(CBP_ERR_LIMIT, "profile length must be < 65536");
+        if ((long long)dists[p] != acc && !(P == 1))
+            throw Error(CBP_ERR_ARG, "profile offsets (pps2DDist) do not follow the lengths");
+        st.h_pstart[p] = acc;
+        acc += lens[p];
+    }
+    if ((size_t)acc != N) throw Error(CBP_ERR_ARG, "sum of profile lengths differs from #positions");
+
+    // packed distance lists
+    std::vector<uint8_t> dst((size_t)N * kDstStride);
+    std::vector<uint8_t> dlen(N);
+    const float* dd[100];
+    for (int s = 0; s < 100; s++) dd[s] = reinterpret_cast<const float*>(beg[fDD + s]);
+    std::string perr;
+    std::mutex emu;
+    parallel_for((long long)N, [&](long long a, long long b) {
+        for (long long n = a; n < b; n++) {
+            const int cnt = (int)dd[0][n];
+            uint8_t* o = dst.data() + (size_t)n * kDstStride;
+            if (cnt < 0 || cnt > kMaxDst) {
+                std::lock_guard<std::mutex> g(emu);
+                perr = "distance count out of range at position " + std::to_string(n);
+                return;
+            }
+            dlen[n] = (uint8_t)cnt;
+            int k = 0;
+            for (; k < cnt; k++) {
+                int v = (int)dd[k + 1][n];
+                if (v < 0) {
+                    std::lock_guard<std::mutex> g(emu);
+                    perr = "negative distance at position " + std::to_string(n);
+                    return;
+                }
+                o[k] = (uint8_t)(v == 255 ? kDstNoData : (v < 20 ? v : 20));
+            }
+            for (; k < kDstStride; k++) o[k] = (uint8_t)kDstNoData;
+        }
+    });
+    if (!perr.empty()) throw Error(CBP_ERR_ARG, perr);
+
+    // profile index of every position, derived from the lengths (the
+    // pmv2DAddrPro field is not trusted for addressing)
+    std::vector<int> pro(N);
+    for (size_t p = 0; p < P; p++)
+        std::fill(pro.begin() + st.h_pstart[p], pro.begin() + st.h_pstart[p] + lens[p], (int)p);
+
+    auto up = [&](DevBuf& b, const void* src, size_t bytes) {
+        b.reserve(std::max<size_t>(bytes, 16));
+        CBP_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, stream));
+    };
+    auto up_rows = [&](DevBuf& b, int f0, int nrows, size_t row_elems, size_t esz) {
+        b.reserve(std::max<size_t>(nrows * row_elems * esz, 16));
+        for (int r = 0; r < nrows; r++)
+            CBP_CUDA(cudaMemcpyAsync(b.as<char>() + r * row_elems * esz, beg[f0 + r], row_elems * esz,
+                                     cudaMemcpyHostToDevice, stream));
+    };
+    up_rows(st.tf, fTF, kNAA, N, sizeof(float));
+    up_rows(st.ss, fSS, kNSS, N, sizeof(float));
+    up_rows(st.trn, fTrn, kNTrn, N + P, sizeof(float));
+    up_rows(st.bkg, fBkg, kNAA, P, sizeof(float));
+    up(st.eno, beg[fENO], P * sizeof(float));
+    up(st.plen, lens, P * sizeof(int));
+    up(st.pstart, st.h_pstart.data(), P * sizeof(long long));
+    up(st.pro, pro.data(), N * sizeof(int));
+    up(st.aa, beg[fAA], N);
+    up(st.sss, beg[fSSstate], N);
+    up(st.dst, dst.data(), dst.size());
+    up(st.dstlen, dlen.data(), N);
+    CBP_CUDA(cudaStreamSynchronize(stream));
+
+    ProfilesDev& v = st.view;
+    v.N = (long long)N; v.P = (int)P;
+    v.tf = st.tf.as<float>(); v.ss = st.ss.as<float>();
+    v.dst = st.dst.as<uint8_t>(); v.dstlen = st.dstlen.as<uint8_t>();
+    v.trn = st.trn.as<float>(); v.bkg = st.bkg.as<float>(); v.eno = st.eno.as<float>();
+    v.plen = st.plen.as<int>(); v.pstart = st.pstart.as<long long>();
+    v.pro = st.pro.as<int>(); v.aa = st.aa.as<int8_t>(); v.sss = st.sss.as<int8_t>();
+}
+
+void check_ctx(cbp_context* c)
+{
+    if (!c) throw Error(CBP_ERR_ARG, "null context");
+    CBP_CUDA(cudaSetDevice(c->device));
+}
+
+// Slabs of whole profiles whose score matrices fit the working budget.
+struct Slab { int p0, p1; long long col0; int ncols; };
+
+std::vector<Slab> plan_slabs(const cbp_context* c, int Lq)
+{
+    const ProfilesStore& db = c->db;
+    const int P = (int)db.h_plen.size();
+    // bytes per slab position: scores + modscores per query position
+    const size_t per_pos = (size_t)Lq * 8 + 64;
+    size_t cap = c->mem_budget / per_pos;
+    if (c->max_slab_positions) cap = std::min(cap, c->max_slab_positions);
+    cap = std::min<size_t>(cap, (size_t)1 << 30);
+    std::vector<Slab> out;
+    int p = 0;
+    while (p < P) {
+        long long start = db.h_pstart[p];
+        int q = p;
+        long long n = 0;
+        while (q < P && (size_t)(n + db.h_plen[q]) <= cap) { n += db.h_plen[q]; q++; }
+        if (q == p) {
+            if (cap < (size_t)db.h_plen[p])
+                throw Error(CBP_ERR_MEMORY, "working memory too small for one profile of length " +
+                                                std::to_string(db.h_plen[p]));
+        }
+        out.push_back({p, q, start, (int)n});
+        p = q;
+    }
+    return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cbp_default_options(cbp_options* o)
+{
+    if (!o) return;
+    o->ssswgt = 0.12f;
+    o->cvswgt = 0.0f;
+    o->ddmswgt = 0.2f;
+    o->dstsegm = 6;
+    o->mapaln = 1;
+    o->minpp = 0.28f;
+    o->ssemodel = 2;
+    o->x_uninf = 1;
+    o->eval = 10.0f;
+    o->nohits = 700;
+    o->noalns = 700;
+}
+
+const char* cbp_last_error(void) { return g_last_error.c_str(); }
+
+int cbp_create(int device, const cbp_options* opt, const float* ss_table, size_t dev_mem_bytes,
+               cbp_context** out)
+{
+    return guarded([&] {
+        if (!out) throw Error(CBP_ERR_ARG, "null output pointer");
+        *out = nullptr;
+        if (!opt || !ss_table) throw Error(CBP_ERR_ARG, "null options or SS table");
+        if (opt->cvswgt != 0.0f)
+            throw Error(CBP_ERR_ARG, "CVSWGT > 0 (context-vector term) is not supported");
+        if (!(opt->ssswgt > 0.0f) || opt->ssswgt >= 1.0f)
+            throw Error(CBP_ERR_ARG, "SSSWGT must be in (0,1)");
+        if (opt->ddmswgt < 0.0f || opt->ddmswgt >= 1.0f) throw Error(CBP_ERR_ARG, "DDMSWGT must be in [0,1)");
+        if (opt->dstsegm < 1 || opt->dstsegm > 20) throw Error(CBP_ERR_ARG, "DSTSEGM must be in [1,20]");
+        int ndev = 0;
+        CBP_CUDA(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev) throw Error(CBP_ERR_ARG, "invalid device");
+        CBP_CUDA(cudaSetDevice(device));
+        auto* c = new cbp_context();
+        try {
+            c->device = device;
+            c->opt = *opt;
+            CBP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            for (auto& e : c->ev) CBP_CUDA(cudaEventCreate(&e));
+            std::memcpy(c->sstab_h, ss_table, sizeof(c->sstab_h));
+            build_dms_table(c->dmstab_h);
+            c->sstab.reserve(sizeof(c->sstab_h));
+            c->dmstab.reserve(sizeof(c->dmstab_h));
+            CBP_CUDA(cudaMemcpy(c->sstab.p, c->sstab_h, sizeof(c->sstab_h), cudaMemcpyHostToDevice));
+            CBP_CUDA(cudaMemcpy(c->dmstab.p, c->dmstab_h, sizeof(c->dmstab_h), cudaMemcpyHostToDevice));
+            size_t fr = 0, tot = 0;
+            CBP_CUDA(cudaMemGetInfo(&fr, &tot));
+            c->mem_budget = dev_mem_bytes ? dev_mem_bytes : (size_t)(0.7 * (double)fr);
+        } catch (...) {
+            cbp_destroy(c);
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int cbp_destroy(cbp_context* c)
+{
+    if (!c) return CBP_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->db.release();
+    c->query.release();
+    c->scores.release();
+    c->modscores.release();
+    c->sstab.release();
+    c->dmstab.release();
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CBP_OK;
+}
+
+int cbp_set_db_details(cbp_context* c, uint64_t db_len, size_t n_seqs)
+{
+    return guarded([&] { check_ctx(c); c->db_len = db_len; c->n_seqs = n_seqs; });
+}
+
+int cbp_set_query_len(cbp_context* c, size_t qlen)
+{
+    return guarded([&] { check_ctx(c); c->query_len = qlen; });
+}
+
+int cbp_set_score_threshold(cbp_context* c, float t)
+{
+    return guarded([&] { check_ctx(c); c->score_thld = t; });
+}
+
+int cbp_set_logE_threshold(cbp_context* c, float t)
+{
+    return guarded([&] { check_ctx(c); c->logE_thld = t; });
+}
+
+int cbp_set_max_slab_positions(cbp_context* c, size_t n)
+{
+    return guarded([&] { check_ctx(c); c->max_slab_positions = n; });
+}
+
+int cbp_transfer_chunk(cbp_context* c, char* const* beg, char* const* end, const size_t*)
+{
+    return guarded([&] {
+        check_ctx(c);
+        c->have_db = false;
+        upload_profiles(c->db, beg, end, c->stream);
+        c->have_db = true;
+    });
+}
+
+int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* const* qbeg,
+                char* const* qend)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!c->have_db) throw Error(CBP_ERR_STATE, "no database chunk transferred");
+        upload_profiles(c->query, qbeg, qend, c->stream);
+        const int Lq = (int)c->query.view.N;
+        if (c->query.view.P != 1) throw Error(CBP_ERR_ARG, "the query field tables must hold one profile");
+        if ((size_t)Lq != query_len) throw Error(CBP_ERR_ARG, "query_len differs from the query profile length");
+        c->launches = 0;
+        for (float& m : c->stage_ms) m = 0.f;
+
+        std::vector<Slab> slabs = plan_slabs(c, Lq);
+        size_t maxcols = 0;
+        for (const Slab& s : slabs) maxcols = std::max(maxcols, (size_t)align_up(s.ncols, 32));
+        c->scores.reserve((size_t)Lq * maxcols * sizeof(float));
+        c->modscores.reserve((size_t)Lq * maxcols * sizeof(float));
+
+        for (const Slab& s : slabs) {
+            ScoreArgs a;
+            a.q = c->query.view;
+            a.db = c->db.view;
+            a.col0 = s.col0;
+            a.ncols = s.ncols;
+            a.ld = align_up(s.ncols, 32);
+            a.Lq = Lq;
+            a.ssswgt = c->opt.ssswgt;
+            a.ddmswgt = c->opt.ddmswgt;
+            a.initshift = c->opt.mapaln ? 0.002f : 0.0003f;
+            a.ddmsshift = 0.2f * c->opt.ddmswgt;
+            a.dstsegm = c->opt.dstsegm;
+            a.sstab = c->sstab.as<float>();
+            a.dmstab = c->dmstab.as<float>();
+            a.scores = c->scores.as<float>();
+            a.modscores = c->modscores.as<float>();
+            CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
+            launch_score_matrix(a, c->stream);
+            c->launches++;
+            CBP_CUDA(cudaEventRecord(c->ev[1], c->stream));
+            CBP_CUDA(cudaEventSynchronize(c->ev[1]));
+            float ms = 0.f;
+            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+            c->stage_ms[0] += ms;
+            c->last_col0 = s.col0;
+            c->last_ncols = s.ncols;
+            c->last_ld = a.ld;
+            c->last_first_profile = s.p0;
+            c->last_Lq = Lq;
+        }
+        CBP_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int cbp_wait_idle(cbp_context* c)
+{
+    return guarded([&] { check_ctx(c); CBP_CUDA(cudaStreamSynchronize(c->stream)); });
+}
+
+int cbp_read_score_matrix(cbp_context* c, float* scores, float* modscores, size_t ld, size_t* ncols,
+                          size_t* first_profile)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!c->last_Lq) throw Error(CBP_ERR_STATE, "no processed query");
+        if (ld < (size_t)c->last_ncols) throw Error(CBP_ERR_ARG, "ld smaller than the slab width");
+        if (ncols) *ncols = (size_t)c->last_ncols;
+        if (first_profile) *first_profile = (size_t)c->last_first_profile;
+        const size_t w = (size_t)c->last_ncols * sizeof(float);
+        if (scores)
+            CBP_CUDA(cudaMemcpy2D(scores, ld * sizeof(float), c->scores.p, c->last_ld * sizeof(float), w,
+                                  c->last_Lq, cudaMemcpyDeviceToHost));
+        if (modscores)
+            CBP_CUDA(cudaMemcpy2D(modscores, ld * sizeof(float), c->modscores.p, c->last_ld * sizeof(float),
+                                  w, c->last_Lq, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cbp_stage_times(cbp_context* c, float* ms, int n)
+{
+    if (!c || !ms) return 0;
+    int k = std::min(n, 6);
+    for (int i = 0; i < k; i++) ms[i] = c->stage_ms[i];
+    return k;
+}
+
+int cbp_launch_count(cbp_context* c, uint64_t* launches)
+{
+    return guarded([&] {
+        if (!c || !launches) throw Error(CBP_ERR_ARG, "null argument");
+        *launches = c->launches;
+    });
+}
+
+}  // extern "C"

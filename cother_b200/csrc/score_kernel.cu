@@ -1,0 +1,301 @@
+// Batch score matrix: profile-profile + secondary structure + distance
+// distribution match score (DDMS) for every (query position, database
+// position) cell of a slab, in ONE kernel.
+//
+// The reference computes the three terms in three kernels that add into the
+// output with atomics (src/libmycu/cusco/CuBatchScoreMatrix.cu:236-396:
+// CalcSM_Init_SMEMUnroll2x, CalcSM_SSSS_SMEMUnroll2x,
+// CalcSM_DDMS2S_SMEMUnroll2x_h2). Here one thread owns one database
+// position (lane) and walks a strip of query positions, adding the terms in
+// the reference's order -- (init + SS) + DDMS -- and writing each cell once.
+//
+// DDMS dominates the cost (~550 segment-DP steps per cell for 99-distance
+// lists); it is CUDA-core ALU-bound, so the kernel is shaped for issue
+// efficiency: byte-packed distance lists in shared memory (odd word stride,
+// conflict-free for lanes in step), a 22x22 pair-score table in shared
+// memory, and one code path for upper and lower diagonals.
+#include "common.cuh"
+#include "cbmath.cuh"
+#include "layout.h"
+#include "score_kernel.cuh"
+
+namespace cbp {
+
+namespace {
+
+constexpr int kCols = 32;          // database positions per block (one per lane)
+constexpr int kWarps = 4;
+constexpr int kThreads = kCols * kWarps;
+constexpr int kRows = 16;          // query positions per block
+constexpr int kElems = 104;        // list elements held per position (99 + overrun)
+constexpr int kDbStride = 108;     // bytes per database list in shared memory (27 words)
+
+// Top-3 register of non-intersecting segments
+// (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s.cuh:182-251). Coordinates
+// are packed [QB QE PB PE]; two segments intersect when their query OR
+// their database ranges overlap (ddms2s.cuh:162-173).
+__device__ __forceinline__ bool coords_intersect(uint32_t c1, uint32_t c2)
+{
+    uint32_t mx = __vmaxu4(c1, c2);
+    uint32_t mn = __vminu4(c1, c2);
+    return ((mn >> 16) & 0xffu) >= ((mx >> 24) & 0xffu) || (mn & 0xffu) >= ((mx >> 8) & 0xffu);
+}
+
+__device__ __forceinline__ void register_max(float (&ms)[3], uint32_t (&mc)[3], float s, uint32_t c)
+{
+    if (ms[0] <= s) {
+        ms[2] = ms[1]; mc[2] = mc[1];
+        ms[1] = ms[0]; mc[1] = mc[0];
+        ms[0] = s; mc[0] = c;
+        if (ms[1] != 0.0f && coords_intersect(mc[0], mc[1])) ms[1] = 0.0f;
+        if (ms[2] != 0.0f && coords_intersect(mc[0], mc[2])) ms[2] = 0.0f;
+        if (ms[1] == 0.0f) { ms[1] = ms[2]; mc[1] = mc[2]; ms[2] = 0.0f; }
+    } else if (ms[1] <= s) {
+        if (coords_intersect(c, mc[0])) return;
+        ms[2] = ms[1]; mc[2] = mc[1];
+        ms[1] = s; mc[1] = c;
+        if (coords_intersect(mc[1], mc[2])) ms[2] = 0.0f;
+    } else if (ms[2] <= s) {
+        if (coords_intersect(c, mc[0]) || coords_intersect(c, mc[1])) return;
+        ms[2] = s; mc[2] = c;
+    }
+}
+
+// One diagonal of the DDMS segment DP. Elements e = 0,1,... pair query list
+// element oq+e with database list element od+e (upper diagonals: oq = 0,
+// od = j; lower: oq = i, od = 0). Pair scores at even offsets within each
+// 4-step are table values, odd ones the mean of their neighbours
+// (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:184-198); a segment
+// restarts when the running sum has fallen to zero, and the best segment of
+// length >= DSTSEGM ending in each 4-step is offered to the top-3 register
+// (ddms2s_h2.cuh:124-176, 288-396).
+__device__ __forceinline__ void ddms_diagonal(
+    const uint8_t* __restrict__ q, const uint8_t* __restrict__ d,
+    const float* __restrict__ T, int lim, int oq, int od, int segm1,
+    float (&ms)[3], uint32_t (&mc)[3])
+{
+    float s0 = T[q[0] * kDstCard + d[0]];
+    float segsco = hmax(s0, 0.0f);
+    int segb = 0;
+    const uint32_t cbase = ((uint32_t)oq << 24) | ((uint32_t)oq << 16) | ((uint32_t)od << 8) | (uint32_t)od;
+    for (int x = 0; x < lim; x += 4) {
+        const float s2 = T[q[x + 2] * kDstCard + d[x + 2]];
+        const float s4 = T[q[x + 4] * kDstCard + d[x + 4]];
+        const float s1 = 0.5f * (s0 + s2);
+        const float s3 = 0.5f * (s2 + s4);
+        float scom = 0.0f;
+        int bb = 0, be = 0;
+#define CBP_DDMS_UPD(S, K)                                             \
+        {                                                              \
+            const int e = x + (K);                                     \
+            if (segsco == 0.0f) segb = e;                              \
+            segsco = hmax(segsco + (S), 0.0f);                         \
+            if (scom < segsco && segb + segm1 <= e) {                  \
+                scom = segsco; bb = segb; be = e;                      \
+            }                                                          \
+        }
+        CBP_DDMS_UPD(s1, 1)
+        CBP_DDMS_UPD(s2, 2)
+        CBP_DDMS_UPD(s3, 3)
+        CBP_DDMS_UPD(s4, 4)
+#undef CBP_DDMS_UPD
+        if (scom != 0.0f) {
+            const uint32_t c = cbase + (((uint32_t)bb << 24) | ((uint32_t)be << 16) |
+                                        ((uint32_t)bb << 8) | (uint32_t)be);
+            register_max(ms, mc, scom, c);
+        }
+        s0 = s4;
+    }
+}
+
+// DDMS of one cell (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:433-500).
+__device__ __forceinline__ float ddms_cell(const uint8_t* __restrict__ q, int len1,
+                                           const uint8_t* __restrict__ d, int len2,
+                                           const float* __restrict__ T, int dstsegm)
+{
+    float ms[3] = {0.0f, 0.0f, 0.0f};
+    uint32_t mc[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
+    const int segm1 = dstsegm - 1;
+    for (int j = len2 >> 2; 0 <= j; j -= 2)
+        ddms_diagonal(q, d + j, T, min(len1, len2 - j), 0, j, segm1, ms, mc);
+    for (int i = len1 >> 2; 0 < i; i -= 2)
+        ddms_diagonal(q + i, d, T, min(len2, len1 - i), i, 0, segm1, ms, mc);
+    float sum = 0.0f;
+    sum = sum + ms[0];
+    sum = sum + ms[1];
+    sum = sum + ms[2];
+    return sum;
+}
+
+__global__ void __launch_bounds__(kThreads)
+score_matrix_kernel(const ScoreArgs a)
+{
+    __shared__ float s_dms[kDstCard * kDstCard];
+    __shared__ float s_sst[kSSCard * kSSCard];
+    __shared__ __align__(16) uint8_t s_dbe[kCols * kDbStride];
+    __shared__ __align__(16) uint8_t s_qe[kRows * kElems];
+    __shared__ float s_dtf[kNAA][kCols];
+    __shared__ float s_dbg[kNAA][kCols];
+    __shared__ float s_dss[kNSS][kCols];
+    __shared__ float s_qtf[kRows][kNAA + 1];
+    __shared__ float s_qss[kRows][kNSS];
+    __shared__ float s_qbg[kNAA];
+    __shared__ int s_dlen[kCols];
+    __shared__ int s_qlen[kRows];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int colb = blockIdx.x * kCols;
+    const int rowb = blockIdx.y * kRows;
+    const long long N = a.db.N;
+
+    for (int i = tid; i < kDstCard * kDstCard; i += kThreads) s_dms[i] = a.dmstab[i];
+    for (int i = tid; i < kSSCard * kSSCard; i += kThreads) s_sst[i] = a.sstab[i];
+
+    // database columns of this block
+    const int col = colb + lane;
+    const bool cvalid = col < a.ncols;
+    const long long gpos = a.col0 + col;
+    if (cvalid) {
+        const int p = a.db.pro[gpos];
+        for (int k = warp; k < kNAA; k += kWarps) {
+            s_dtf[k][lane] = a.db.tf[(long long)k * N + gpos];
+            s_dbg[k][lane] = a.db.bkg[(long long)k * a.db.P + p];
+        }
+        if (warp < kNSS) s_dss[warp][lane] = a.db.ss[(long long)warp * N + gpos];
+        if (warp == kNSS) s_dlen[lane] = a.db.dstlen[gpos];
+    } else if (warp == kNSS) {
+        s_dlen[lane] = 0;
+    }
+    // distance lists: 32 columns x 104 bytes, in 16-byte pieces
+    for (int idx = tid; idx < kCols * 7; idx += kThreads) {
+        const int c = idx / 7, piece = idx - c * 7;
+        uint4 v;
+        if (colb + c < a.ncols) {
+            v = *reinterpret_cast<const uint4*>(a.db.dst + (a.col0 + colb + c) * kDstStride + piece * 16);
+        } else {
+            const uint32_t f = 0x15151515u;  // kDstNoData in every byte
+            v = make_uint4(f, f, f, f);
+        }
+        uint32_t* dstw = reinterpret_cast<uint32_t*>(s_dbe + c * kDbStride + piece * 16);
+        dstw[0] = v.x; dstw[1] = v.y; dstw[2] = v.z;
+        if (piece < 6) dstw[3] = v.w;   // piece 6 covers bytes 96..107 only
+    }
+    // query rows of this block
+    for (int idx = tid; idx < kRows * kNAA; idx += kThreads) {
+        const int r = idx / kNAA, k = idx - r * kNAA;
+        const int row = rowb + r;
+        s_qtf[r][k] = row < a.Lq ? a.q.tf[(long long)k * a.q.N + row] : 0.0f;
+    }
+    for (int idx = tid; idx < kRows * kNSS; idx += kThreads) {
+        const int r = idx / kNSS, k = idx - r * kNSS;
+        const int row = rowb + r;
+        s_qss[r][k] = row < a.Lq ? a.q.ss[(long long)k * a.q.N + row] : 0.0f;
+    }
+    if (tid < kNAA) s_qbg[tid] = a.q.bkg[tid];
+    if (tid < kRows) s_qlen[tid] = (rowb + tid < a.Lq) ? a.q.dstlen[rowb + tid] : 0;
+    for (int idx = tid; idx < kRows * (kElems / 4); idx += kThreads) {
+        const int r = idx / (kElems / 4), w = idx - r * (kElems / 4);
+        const int row = rowb + r;
+        uint32_t v = 0x15151515u;
+        if (row < a.Lq) v = *reinterpret_cast<const uint32_t*>(a.q.dst + (long long)row * kDstStride + 4 * w);
+        reinterpret_cast<uint32_t*>(s_qe + r * kElems)[w] = v;
+    }
+    __syncthreads();
+
+    if (!cvalid) return;  // no block-wide synchronisation below
+
+    const int dlen = s_dlen[lane];
+    const uint8_t* de = s_dbe + lane * kDbStride;
+    const float dss0 = s_dss[0][lane], dss1 = s_dss[1][lane], dss2 = s_dss[2][lane];
+
+    for (int r = warp; r < kRows; r += kWarps) {
+        const int row = rowb + r;
+        if (row >= a.Lq) break;
+
+        // profile-profile term (CuBatchScoreMatrix_Init.cu:159-186)
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < kNAA; k++) {
+            const float num = s_qtf[r][k] * s_dtf[k][lane];
+            const float den = 0.5f * (s_qbg[k] + s_dbg[k][lane]);
+            acc = acc + __fdiv_rn(num, den);
+        }
+        float s = cb_logf(acc) - a.initshift;
+        float mod = 0.0f;
+
+        // SS term (CuBatchScoreMatrix_ssss.cu:209-279)
+        if (a.ssswgt > 0.0f) {
+            float ss = 0.0f;
+            const float dsv[3] = {dss0, dss1, dss2};
+#pragma unroll
+            for (int i = 0; i < kNSS; i++) {
+                const float f1 = s_qss[r][i];
+                const int ri = i * 10 + (int)(f1 * 9.999f);
+#pragma unroll
+                for (int j = 0; j < kNSS; j++) {
+                    const float f2 = dsv[j];
+                    const int cj = j * 10 + (int)(f2 * 9.999f);
+                    ss = __fmaf_rn(f1 * f2, s_sst[ri * kSSCard + cj], ss);
+                }
+            }
+            if (-99.0f < ss) {
+                ss = __fmaf_rn((s_qss[r][2] + 0.1f) * (dss2 + 0.1f), 0.1111111f, ss);
+                ss = ss - 0.05f;
+                ss = ss * a.ssswgt;
+            }
+            s = s + ss;
+            mod = ss;
+        }
+
+        // DDMS term (CuBatchScoreMatrix_ddms2s_h2.cu:158-186)
+        if (a.ddmswgt > 0.0f) {
+            const int qlen = s_qlen[r];
+            if (qlen >= a.dstsegm && dlen >= a.dstsegm) {
+                const float sum = ddms_cell(s_qe + r * kElems, qlen, de, dlen, s_dms, a.dstsegm);
+                const float dm = __fmaf_rn(0.053f * 16.0f, sum, -1.235f) * a.ddmswgt;
+                if (dm != 0.0f) {
+                    s = s + dm;
+                    mod = mod + (dm - a.ddmsshift);
+                }
+            }
+        }
+        const long long o = (long long)row * a.ld + col;
+        a.scores[o] = s;
+        a.modscores[o] = mod;
+    }
+}
+
+}  // namespace
+
+void launch_score_matrix(const ScoreArgs& a, cudaStream_t stream)
+{
+    if (a.ncols <= 0 || a.Lq <= 0) return;
+    dim3 grid((unsigned)ceil_div(a.ncols, kCols), (unsigned)ceil_div(a.Lq, kRows));
+    score_matrix_kernel<<<grid, kThreads, 0, stream>>>(a);
+    CBP_CHECK_LAUNCH();
+}
+
+// Pair-score table over packed distance codes (0..20 saturated, 21 = no
+// data), computed on the host with each operation rounded separately, as
+// the reference's own CPU table does (cother-scores-optimizer/dstable.h:339-365,
+// constants src/libmycu/cupro/SerializedDstMatchScoresAttr.h:29-31).
+void build_dms_table(float* T)
+{
+    volatile float s00 = 0.35f, s200 = -0.4f, inv = 0.05f;
+    for (int a1 = 0; a1 < kDstCard; a1++)
+        for (int a2 = 0; a2 < kDstCard; a2++) {
+            if (a1 == kDstNoData || a2 == kDstNoData) { T[a1 * kDstCard + a2] = -1.0f; continue; }
+            int d1 = a1 > a2 ? a1 : a2, d2 = a1 > a2 ? a2 : a1;
+            volatile float t = (float)d2 * s200;
+            volatile float t2 = t * inv;
+            volatile float intpt = s00 - t2;
+            volatile float sl0 = s200 - s00;
+            volatile float slope = sl0 * inv;
+            volatile float prod = (float)d1 * slope;
+            T[a1 * kDstCard + a2] = prod + intpt;
+        }
+}
+
+}  // namespace cbp

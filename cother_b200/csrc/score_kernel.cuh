@@ -1,0 +1,27 @@
+// Score-matrix stage interface.
+#pragma once
+
+#include <cuda_runtime.h>
+#include "layout.h"
+
+namespace cbp {
+
+struct ScoreArgs {
+    ProfilesDev q;        // query profile
+    ProfilesDev db;       // resident database chunk
+    long long col0 = 0;   // first chunk position of the slab
+    int ncols = 0;        // slab positions
+    long long ld = 0;     // leading dimension of the outputs
+    int Lq = 0;
+    float ssswgt = 0.f, ddmswgt = 0.f, initshift = 0.f, ddmsshift = 0.f;
+    int dstsegm = 6;
+    const float* sstab = nullptr;   // [30][30]
+    const float* dmstab = nullptr;  // [22][22]
+    float* scores = nullptr;        // [Lq][ld]
+    float* modscores = nullptr;     // [Lq][ld]
+};
+
+void launch_score_matrix(const ScoreArgs& a, cudaStream_t stream);
+void build_dms_table(float* T);
+
+}  // namespace cbp

@@ -1,0 +1,135 @@
+"""Seeded synthetic query and database profiles.
+
+The workloads stand in for real profile databases (none can be downloaded
+here). Shapes and value distributions follow the benchmark configurations
+of the search path:
+
+* query profiles carry *predicted* C-beta distance distributions (17 bins
+  over 2-20 A, Dirichlet(0.3)) for every pair 3 <= |i-j| < window;
+* database profiles carry *observed* distances from a C-beta random walk
+  with 3.8 A steps;
+* target frequencies are Dirichlet(0.5) draws mixed with the profile
+  background, SS probabilities Dirichlet(1), the effective number of
+  observations uniform in [1, 14];
+* database lengths are lognormal (sigma 0.5) clipped to a range.
+
+The heavy lifting (distance lists) runs in ``libcbsynth.so`` with one
+random stream per profile, so results do not depend on the thread count.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+from .profiles import NDSTSLOTS, NSSSTATES, NTRN, NUMAA, ProfileSet
+
+_lib = None
+
+
+def _synth_lib():
+    global _lib
+    if _lib is None:
+        path = _build.LIB_SYNTH
+        if not os.path.exists(path):
+            _build.build_synth()
+        lib = ctypes.CDLL(path)
+        lib.cbs_generate.restype = ctypes.c_int
+        lib.cbs_generate.argtypes = [
+            ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_ulonglong,
+            ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_int,
+        ]
+        _lib = lib
+    return _lib
+
+
+def global_background() -> np.ndarray:
+    """Fixed amino-acid background shared by all synthetic profiles."""
+    rng = np.random.default_rng(20240917)
+    return rng.dirichlet(np.full(NUMAA, 40.0))
+
+
+def make_profiles(lens, seed: int, predicted: bool, window: int = 64,
+                  prb_thld: float = 0.05, nthreads: int | None = None) -> ProfileSet:
+    """Generate profiles of the given lengths."""
+    lens = np.ascontiguousarray(np.asarray(lens, dtype=np.int32))
+    P = int(len(lens))
+    N = int(lens.sum(dtype=np.int64))
+    starts = np.zeros(P, dtype=np.int64)
+    if P > 1:
+        starts[1:] = np.cumsum(lens[:-1], dtype=np.int64)
+    bkg = np.zeros((NUMAA, P), np.float32)
+    eno = np.zeros(P, np.float32)
+    trn = np.zeros((NTRN, N + P), np.float32)
+    tf = np.zeros((NUMAA, N), np.float32)
+    ss = np.zeros((NSSSTATES, N), np.float32)
+    ssstate = np.zeros(N, np.int8)
+    aa = np.zeros(N, np.int8)
+    dd = np.zeros((NDSTSLOTS, N), np.float32)
+    addrpro = np.zeros(N, np.int32)
+    gb = np.ascontiguousarray(global_background(), dtype=np.float64)
+    if nthreads is None:
+        nthreads = max(1, min(os.cpu_count() or 1, 32))
+    rc = _synth_lib().cbs_generate(
+        P, N, lens.ctypes.data, starts.ctypes.data,
+        1 if predicted else 0, int(window), float(prb_thld), int(seed) & 0xFFFFFFFFFFFFFFFF,
+        gb.ctypes.data,
+        bkg.ctypes.data, eno.ctypes.data, trn.ctypes.data, tf.ctypes.data, ss.ctypes.data,
+        ssstate.ctypes.data, aa.ctypes.data, dd.ctypes.data, addrpro.ctypes.data,
+        int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"cbs_generate failed ({rc})")
+    return ProfileSet(lens=lens, bkg=bkg, eno=eno, trn=trn, tf=tf, dd=dd, ss=ss,
+                      addrpro=addrpro, aa=aa, ssstate=ssstate,
+                      names=[f"synth{seed}_{i}" for i in range(P)])
+
+
+def lognormal_lengths(n: int, median: float, lo: int, hi: int, seed: int,
+                      sigma: float = 0.5) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    x = rng.lognormal(mean=np.log(median), sigma=sigma, size=n)
+    return np.clip(np.rint(x), lo, hi).astype(np.int32)
+
+
+def uniform_lengths(n: int, lo: int, hi: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.integers(lo, hi + 1, size=n).astype(np.int32)
+
+
+# Workloads of the benchmark configurations. Each entry gives the query
+# lengths, the database length law and the distance window.
+WORKLOADS = {
+    # 1 query of length 200 vs 1,000 profiles, lognormal median 180 in [30,600]
+    "q200_db1k": dict(qlens=[200], ndb=1000, law=("lognormal", 180, 30, 600), window=64),
+    # 1 query of length 400 vs 50,000 profiles, lognormal median 220 in [30,1500]
+    "q400_db50k": dict(qlens=[400], ndb=50000, law=("lognormal", 220, 30, 1500), window=64),
+    # query-length sweep over the 50,000-profile database
+    "qsweep_db50k": dict(qlens=[64, 256, 1024], ndb=50000, law=("lognormal", 220, 30, 1500), window=64),
+    # 1 query of length 1,500 vs 20,000 profiles of length U(500,1500), window 128
+    "q1500_db20k": dict(qlens=[1500], ndb=20000, law=("uniform", 500, 1500), window=128),
+}
+
+
+def db_lengths(name: str, seed: int = 7, ndb: int | None = None) -> np.ndarray:
+    w = WORKLOADS[name]
+    n = w["ndb"] if ndb is None else ndb
+    law = w["law"]
+    if law[0] == "lognormal":
+        return lognormal_lengths(n, law[1], law[2], law[3], seed)
+    return uniform_lengths(n, law[1], law[2], seed)
+
+
+def make_workload(name: str, seed: int = 7, ndb: int | None = None, qindex: int = 0):
+    """(query ProfileSet, database ProfileSet) for a named workload."""
+    w = WORKLOADS[name]
+    lens = db_lengths(name, seed, ndb)
+    db = make_profiles(lens, seed=seed * 1000 + 1, predicted=False, window=w["window"])
+    q = make_profiles([w["qlens"][qindex]], seed=seed * 1000 + 2 + qindex, predicted=True,
+                      window=w["window"])
+    return q, db

@@ -1,0 +1,152 @@
+/*
+ * cother_b200 -- B200-native (sm_100a) search path of COTHER behind a C ABI.
+ *
+ * One context corresponds to one instance of the reference's per-worker
+ * driver class CuBatchProcessing (src/libmycu/cupro/CuBatchProcessing.cuh:47-244):
+ * it owns a CUDA stream on one GPU, a GPU-resident database chunk and the
+ * working memory of the pipeline
+ *
+ *   score matrix (profile-profile + SS + DDMS)
+ *     -> phase-1 gapped local DP + finalization (pass list)
+ *     -> alignment statistics and E-values
+ *     -> phase-2 MAP forward/backward/MAP alignment + finalization
+ *     -> hit records and alignment strings.
+ *
+ * Profile data cross the boundary exactly as in the reference: 181 parallel
+ * structure-of-arrays field arrays given as begin/end pointer tables
+ * (char* pmbeg[181], char* pmend[181]; field order of
+ * src/libmycu/cupro/PM2DVectorFields.h:51-87).
+ *
+ * All functions return 0 on success and a non-zero status otherwise; the
+ * message of the last failure on the calling thread is returned by
+ * cbp_last_error(). No function terminates the process or traps on the
+ * device. A context may be used by one host thread at a time; different
+ * contexts are independent (several may share a GPU).
+ */
+#ifndef COTHER_B200_H
+#define COTHER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CBP_NFIELDS 181          /* pmv2DTotFlds */
+#define CBP_MAX_DST_VALUES 99    /* MAX_N_IR_DISTANCE_VALUES */
+#define CBP_SS_CARD 30           /* cardinality of the SS score table */
+
+/* status codes */
+enum {
+    CBP_OK = 0,
+    CBP_ERR_ARG = 1,       /* invalid argument */
+    CBP_ERR_CUDA = 2,      /* CUDA runtime error */
+    CBP_ERR_STATE = 3,     /* call out of order (e.g. process before transfer) */
+    CBP_ERR_MEMORY = 4,    /* device memory budget exceeded */
+    CBP_ERR_LIMIT = 5      /* input beyond a format limit (e.g. length >= 65536) */
+};
+
+typedef struct cbp_context cbp_context;
+
+/* Options of the path (src/libpro/srcpro/MOptions.cpp:76-147). */
+typedef struct cbp_options {
+    float ssswgt;     /* SSSWGT: weight of the SS score (> 0) */
+    float cvswgt;     /* CVSWGT: context-vector term; must be 0 (term off) */
+    float ddmswgt;    /* DDMSWGT: weight of the DDMS score */
+    int   dstsegm;    /* DSTSEGM: minimum DDMS segment length */
+    int   mapaln;     /* MAPALN: 1 = MAP realignment in phase 2 */
+    float minpp;      /* MINPP: minimum posterior probability */
+    int   ssemodel;   /* SSEMODEL: statistical significance model (0..2) */
+    int   x_uninf;    /* X_UNINF: mask uninformative (X) positions */
+    float eval;       /* EVAL: E-value threshold */
+    int   nohits;     /* NOHITS */
+    int   noalns;     /* NOALNS */
+} cbp_options;
+
+/* Fill *opt with the values of the parity configuration:
+ * SSSWGT=0.12, CVSWGT=0, DDMSWGT=0.2, DSTSEGM=6, MAPALN=1, MINPP=0.28,
+ * SSEMODEL=2, X_UNINF=1, EVAL=10, NOHITS=NOALNS=700. */
+void cbp_default_options(cbp_options* opt);
+
+/* Create a context on `device`.
+ *   ss_table: the SS score table, CBP_SS_CARD x CBP_SS_CARD floats, full
+ *             symmetric (the lower triangle of the reference's env/ssss file);
+ *   dev_mem_bytes: device memory the context may use for working buffers
+ *             (0 = 70% of the free memory at creation).
+ * Replaces CuBatchProcessing::CuBatchProcessing
+ * (src/libmycu/cupro/CuBatchProcessing.cuh:50-58; device heap planning of
+ * src/libmycu/cupro/CuDeviceMemory.cu:285-588). */
+int cbp_create(int device, const cbp_options* opt, const float* ss_table,
+               size_t dev_mem_bytes, cbp_context** ctx);
+
+/* Release all resources (CuBatchProcessing::~CuBatchProcessing). */
+int cbp_destroy(cbp_context* ctx);
+
+/* Database totals used for E-values: residues and sequences of the WHOLE
+ * database, not of the chunk (CuBatchProcessing::SetDbDetails,
+ * src/libmycu/cupro/CuBatchProcessing.cuh:73-76). */
+int cbp_set_db_details(cbp_context* ctx, uint64_t db_len, size_t n_seqs);
+
+/* Query length used for the length adjustment (SetQueryLen, :78-79). */
+int cbp_set_query_len(cbp_context* ctx, size_t query_len);
+
+/* Phase-1 score threshold (SetScoreThreshold, :80-82). */
+int cbp_set_score_threshold(cbp_context* ctx, float threshold);
+
+/* log E-value threshold for phase 2 (SetLogEThreshold, :83-85). */
+int cbp_set_logE_threshold(cbp_context* ctx, float log_threshold);
+
+/* Upload a database chunk and keep it resident until the next call
+ * (CuBatchProcessing::TransferCPMData, :62-71; copy of
+ * src/libmycu/cupro/CuDeviceMemory.cu:1095-1139). `pmbeg`/`pmend` are the
+ * begin/end pointer tables of the chunk's 181 host field arrays; `szfields`
+ * is accepted for interface compatibility and may be NULL. */
+int cbp_transfer_chunk(cbp_context* ctx, char* const* pmbeg, char* const* pmend,
+                       const size_t* szfields);
+
+/* Search one query against the resident chunk
+ * (CuBatchProcessing::ProcessScoreMatrix, :87-99). `qpmbeg`/`qpmend` are
+ * the pointer tables of the query's field arrays (one profile). The call
+ * returns when the results are available through cbp_get_results(). */
+int cbp_process(cbp_context* ctx, int query_serial, size_t query_len,
+                char* const* qpmbeg, char* const* qpmend);
+
+/* Wait until no work of this context is in flight (WaitForIdleChilds). */
+int cbp_wait_idle(cbp_context* ctx);
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char* cbp_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * Inspection of intermediate results of the last cbp_process() call. They
+ * exist for verification and refer to the LAST processed slab of database
+ * profiles (see cbp_set_max_slab_positions).
+ */
+
+/* Copy the score matrices (query positions x slab positions) to host:
+ * scores[r * ld + c] and modscores[r * ld + c] for r < query length and
+ * c < *ncols (the number of slab positions, written on return).
+ * Either output may be NULL; `first_profile` receives the index of the
+ * slab's first profile within the chunk. */
+int cbp_read_score_matrix(cbp_context* ctx, float* scores, float* modscores,
+                          size_t ld, size_t* ncols, size_t* first_profile);
+
+/* Limit the number of database positions processed per slab (0 = plan by
+ * the memory budget). Used to exercise multi-slab processing. */
+int cbp_set_max_slab_positions(cbp_context* ctx, size_t max_positions);
+
+/* Device time in milliseconds of the kernels of the last cbp_process()
+ * call, per stage: [0] score matrix, [1] phase-1 DP, [2] phase-1
+ * finalization, [3] statistics, [4] MAP phase, [5] result assembly.
+ * Returns the number of stages written (<= n). */
+int cbp_stage_times(cbp_context* ctx, float* ms, int n);
+
+/* Number of kernel launches issued by the last cbp_process() call. */
+int cbp_launch_count(cbp_context* ctx, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COTHER_B200_H */

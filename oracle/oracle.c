@@ -1,0 +1,342 @@
+/*
+ * CPU oracle for the COTHER search path -- TEST INFRASTRUCTURE ONLY.
+ * See oracle.h for the rules. Compiled with -ffp-contract=off.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------
+ * orc_logf: natural logarithm of a positive finite float.
+ *
+ * Not a restatement of any library routine: x = m * 2^e with m in
+ * [sqrt(1/2), sqrt(2)), t = (m-1)/(m+1) and log(m) = 2*atanh(t) summed as
+ * the odd power series 2(t + t^3/3 + ... + t^9/9) (|t| <= 0.1716, the next
+ * term is below 1e-9 relative). Every operation is an IEEE single-precision
+ * add, multiply, divide or fused multiply-add, so the CUDA kernels compute
+ * bit-identical values with the same sequence.
+ * The reference takes __logf() of the same argument
+ * (src/libmycu/cusco/CuBatchScoreMatrix_Init.cu:180).
+ */
+float orc_logf(float x)
+{
+    union { float f; uint32_t u; } v = {x};
+    int e = 0;
+    if (v.u < 0x00800000u) {          /* subnormal: scale by 2^23 */
+        v.f = x * 8388608.0f;
+        e = -23;
+    }
+    e += (int)((v.u >> 23) & 0xffu) - 127;
+    v.u = (v.u & 0x007fffffu) | 0x3f800000u;  /* m in [1,2) */
+    float m = v.f;
+    if (m > 1.41421356f) { m = m * 0.5f; e += 1; }
+    float t = (m - 1.0f) / (m + 1.0f);
+    float t2 = t * t;
+    float p = fmaf(t2, 0.11111111f, 0.14285715f);
+    p = fmaf(t2, p, 0.2f);
+    p = fmaf(t2, p, 0.33333334f);
+    float t2x = t + t;
+    float lm = fmaf(t2x * t2, p, t2x);
+    float fe = (float)e;
+    return fmaf(fe, 0.693145751953125f, fmaf(fe, 1.42860677e-06f, lm));
+}
+
+/* ------------------------------------------------------------------------
+ * DDMS pair score with the two-level linear interpolation of the reference
+ * (src/libmycu/cupro/SerializedDstMatchScores.cuh:347-396, constants
+ * src/libmycu/cupro/SerializedDstMatchScoresAttr.h:29-31 and
+ * SerializedDstMatchScores.cuh:19-20): distances saturate at 20
+ * (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:60), 255 scores -1;
+ * with d1 >= d2: score = d1*slope + (0.35 - d2*(-0.4)*0.05),
+ * slope = (-0.4-0.35)*0.05, each operation rounded separately as in the
+ * reference's own CPU table (cother-scores-optimizer/dstable.h:339-365).
+ */
+float orc_dms_pair_score(int d1, int d2)
+{
+    if (d1 == 0xff || d2 == 0xff) return -1.0f;
+    if (d1 > 20) d1 = 20;
+    if (d2 > 20) d2 = 20;
+    if (d1 < d2) { int t = d1; d1 = d2; d2 = t; }
+    float intpt = 0.35f - ((float)d2 * -0.4f) * 0.05f;
+    float slope = (-0.4f - 0.35f) * 0.05f;
+    float prod = (float)d1 * slope;
+    return prod + intpt;
+}
+
+/* ------------------------------------------------------------------------
+ * Top-3 non-intersecting segment register
+ * (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s.cuh:114-251).
+ * Coordinates are packed [QB QE PB PE], one byte each.
+ */
+#define ORC_COORDS(QB, QE, PB, PE) \
+    ((((uint32_t)(QB) & 0xffu) << 24) | (((uint32_t)(QE) & 0xffu) << 16) | \
+     (((uint32_t)(PB) & 0xffu) << 8) | ((uint32_t)(PE) & 0xffu))
+
+static int orc_coords_intersect(uint32_t c1, uint32_t c2)
+{
+    uint32_t mx = 0, mn = 0;
+    for (int b = 0; b < 32; b += 8) {
+        uint32_t x = (c1 >> b) & 0xffu, y = (c2 >> b) & 0xffu;
+        mx |= (x > y ? x : y) << b;
+        mn |= (x < y ? x : y) << b;
+    }
+    return ((mn >> 16) & 0xffu) >= ((mx >> 24) & 0xffu) ||
+           (mn & 0xffu) >= ((mx >> 8) & 0xffu);
+}
+
+static void orc_register_max(float* ms, uint32_t* mc, float segsco, uint32_t segcoords)
+{
+    if (segsco == 0.0f) return;
+    if (ms[0] <= segsco) {
+        ms[2] = ms[1]; mc[2] = mc[1];
+        ms[1] = ms[0]; mc[1] = mc[0];
+        ms[0] = segsco; mc[0] = segcoords;
+        if (ms[1] != 0.0f && orc_coords_intersect(mc[0], mc[1])) ms[1] = 0.0f;
+        if (ms[2] != 0.0f && orc_coords_intersect(mc[0], mc[2])) ms[2] = 0.0f;
+        if (ms[1] == 0.0f) {
+            ms[1] = ms[2]; mc[1] = mc[2];
+            ms[2] = 0.0f;
+        }
+    } else if (ms[1] <= segsco) {
+        if (orc_coords_intersect(segcoords, mc[0])) return;
+        ms[2] = ms[1]; mc[2] = mc[1];
+        ms[1] = segsco; mc[1] = segcoords;
+        if (orc_coords_intersect(mc[1], mc[2])) ms[2] = 0.0f;
+    } else if (ms[2] <= segsco) {
+        if (orc_coords_intersect(segcoords, mc[0]) || orc_coords_intersect(segcoords, mc[1]))
+            return;
+        ms[2] = segsco; mc[2] = segcoords;
+    }
+}
+
+static inline float orc_hmax(float a, float b) { return a < b ? b : a; }
+
+/* list value at 1-based slot k; slots past the count read as no data
+ * (the reference pads its shared-memory copy with 0xff:
+ * src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:91-104) */
+static inline int orc_lv(const uint8_t* lst, int k)
+{
+    int n = lst[0];
+    if (k > n || k >= ORC_NDSTSLOTS) return 0xff;
+    return lst[k];
+}
+
+static inline float orc_S(const uint8_t* q, int kq, const uint8_t* d, int kd)
+{
+    return orc_dms_pair_score(orc_lv(q, kq), orc_lv(d, kd));
+}
+
+/* Upper part: diagonal j of the DP over the two lists
+ * (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:288-340, segment
+ * update :124-147, unrolled reads :184-198). */
+static void orc_diag_upper(const uint8_t* q, const uint8_t* d, int dstsegm, int len1, int len2,
+                           int j, float* ms, uint32_t* mc)
+{
+    float segsco;
+    int segqb = 0, segpb = j;
+    float s[5];
+    s[0] = orc_S(q, 1, d, j + 1);
+    segsco = orc_hmax(s[0], 0.0f);
+    for (int i = 0; i < len1 && j + i < len2; i += 4) {
+        float scom = 0.0f;
+        int im = 0, jim = 0, ib = 0, jib = 0;
+        s[2] = orc_S(q, i + 3, d, j + i + 3);
+        s[4] = orc_S(q, i + 5, d, j + i + 5);
+        s[3] = 0.5f * (s[2] + s[4]);
+        s[1] = 0.5f * (s[0] + s[2]);
+        for (int k = 1; k <= 4; k++) {
+            if (segsco == 0.0f) { segqb = i + k; segpb = j + i + k; }
+            segsco = orc_hmax(segsco + s[k], 0.0f);
+            if (segsco != 0.0f) {
+                if (scom < segsco && dstsegm <= i + k - segqb + 1) {
+                    scom = segsco;
+                    im = i + k; jim = j + i + k;
+                    ib = segqb; jib = segpb;
+                }
+            }
+        }
+        orc_register_max(ms, mc, scom, ORC_COORDS(ib, im, jib, jim));
+        s[0] = s[4];
+    }
+}
+
+/* Lower part: diagonal i (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:345-396,
+ * segment update :153-176). */
+static void orc_diag_lower(const uint8_t* q, const uint8_t* d, int dstsegm, int len1, int len2,
+                           int i, float* ms, uint32_t* mc)
+{
+    float segsco;
+    int segqb = i, segpb = 0;
+    float s[5];
+    s[0] = orc_S(q, i + 1, d, 1);
+    segsco = orc_hmax(s[0], 0.0f);
+    for (int j = 0; j < len2 && i + j < len1; j += 4) {
+        float scom = 0.0f;
+        int ijm = 0, jm = 0, ijb = 0, jb = 0;
+        s[2] = orc_S(q, i + j + 3, d, j + 3);
+        s[4] = orc_S(q, i + j + 5, d, j + 5);
+        s[3] = 0.5f * (s[2] + s[4]);
+        s[1] = 0.5f * (s[0] + s[2]);
+        for (int k = 1; k <= 4; k++) {
+            if (segsco == 0.0f) { segqb = i + j + k; segpb = j + k; }
+            segsco = orc_hmax(segsco + s[k], 0.0f);
+            if (segsco != 0.0f) {
+                if (scom < segsco && dstsegm <= j + k - segpb + 1) {
+                    scom = segsco;
+                    ijm = i + j + k; jm = j + k;
+                    ijb = segqb; jb = segpb;
+                }
+            }
+        }
+        orc_register_max(ms, mc, scom, ORC_COORDS(ijb, ijm, jb, jm));
+        s[0] = s[4];
+    }
+}
+
+/* DDMS for one cell (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:433-500):
+ * band of diagonals j = len2>>2 .. 0 step 2 (upper), i = len1>>2 .. 1 step 2
+ * (lower); score = (0.053*16*sum + (-1.235)) * DDMSWGT. */
+float orc_ddms_cell(const uint8_t* qlist, const uint8_t* dlist, int dstsegm,
+                    float ddmswgt, float* rawsum, int* computed)
+{
+    int len1 = qlist[0], len2 = dlist[0];
+    *rawsum = 0.0f;
+    *computed = 0;
+    if (len1 < dstsegm || len2 < dstsegm) return 0.0f;
+    *computed = 1;
+    float ms[3] = {0.0f, 0.0f, 0.0f};
+    uint32_t mc[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
+    for (int j = len2 >> 2; 0 <= j; j -= 2)
+        orc_diag_upper(qlist, dlist, dstsegm, len1, len2, j, ms, mc);
+    for (int i = len1 >> 2; 0 < i; i -= 2)
+        orc_diag_lower(qlist, dlist, dstsegm, len1, len2, i, ms, mc);
+    float sum = 0.0f;
+    for (int k = 0; k < 3; k++) sum = sum + ms[k];
+    *rawsum = sum;
+    const float slope = 0.053f * 16.0f;
+    float sc = fmaf(slope, sum, -1.235f);
+    return sc * ddmswgt;
+}
+
+/* ------------------------------------------------------------------------
+ * Profile-profile score (src/libmycu/cusco/CuBatchScoreMatrix_Init.cu:159-186):
+ * log( sum_a q_tf[a]*d_tf[a] / (0.5*(q_bkg[a]+d_bkg[a])) ) - shift.
+ * SS score (src/libmycu/cusco/CuBatchScoreMatrix_ssss.cu:209-279,
+ * table index CuBatchScoreMatrix_ssss.cuh:26-31).
+ */
+static float orc_init_score(const float* qtf, long long qstride, const float* qbk,
+                            const float* dtf, long long dstride, const float* dbk, long long bstride,
+                            float shift)
+{
+    float acc = 0.0f;
+    for (int a = 0; a < 20; a++) {
+        float num = qtf[a * qstride] * dtf[a * dstride];
+        float den = 0.5f * (qbk[a] + dbk[a * bstride]);
+        acc = acc + num / den;
+    }
+    return orc_logf(acc) - shift;
+}
+
+static float orc_ss_score(const float* qss, long long qstride, const float* dss, long long dstride,
+                          const float* T, float ssswgt)
+{
+    float acc = 0.0f;
+    for (int i = 0; i < 3; i++) {
+        float f1 = qss[i * qstride];
+        int r = i * 10 + (int)(f1 * 9.999f);
+        for (int j = 0; j < 3; j++) {
+            float f2 = dss[j * dstride];
+            int c = j * 10 + (int)(f2 * 9.999f);
+            acc = fmaf(f1 * f2, T[r * ORC_NOTABLE_SS + c], acc);
+        }
+    }
+    float f1 = qss[2 * qstride], f2 = dss[2 * dstride];
+    if (-99.0f < acc) {
+        acc = fmaf((f1 + 0.1f) * (f2 + 0.1f), 0.1111111f, acc);
+        acc = acc - 0.05f;
+        acc = acc * ssswgt;
+    }
+    return acc;
+}
+
+void orc_score_matrix(int Lq, const float* q_tf, const float* q_bkg, const float* q_ss,
+                      const uint8_t* q_dd,
+                      long long N, int P, const float* d_tf, const float* d_bkg,
+                      const int32_t* d_pro, const float* d_ss, const uint8_t* d_dd,
+                      const float* ss_table, const orc_score_params* prm,
+                      long long col0, long long ncols,
+                      float* scores, float* modscores, long long ld)
+{
+    const float ddmsshift = 0.2f * prm->ddmswgt;
+    for (int r = 0; r < Lq; r++) {
+        for (long long c = col0; c < col0 + ncols; c++) {
+            int p = d_pro[c];
+            float s = orc_init_score(q_tf + r, Lq, q_bkg, d_tf + c, N, d_bkg + p, P, prm->initshift);
+            float ms = 0.0f;
+            if (prm->ssswgt > 0.0f) {
+                float ss = orc_ss_score(q_ss + r, Lq, d_ss + c, N, ss_table, prm->ssswgt);
+                s = s + ss;
+                ms = ss;
+            }
+            if (prm->ddmswgt > 0.0f) {
+                float raw; int comp;
+                float dm = orc_ddms_cell(q_dd + (size_t)r * ORC_NDSTSLOTS,
+                                         d_dd + (size_t)c * ORC_NDSTSLOTS,
+                                         prm->dstsegm, prm->ddmswgt, &raw, &comp);
+                if (comp && dm != 0.0f) {
+                    s = s + dm;
+                    ms = ms + (dm - ddmsshift);
+                }
+            }
+            scores[(size_t)r * ld + (c - col0)] = s;
+            modscores[(size_t)r * ld + (c - col0)] = ms;
+        }
+    }
+}
+
+typedef struct {
+    int Lq; const float *q_tf, *q_bkg, *q_ss; const uint8_t* q_dd;
+    long long N; int P; const float *d_tf, *d_bkg; const int32_t* d_pro;
+    const float* d_ss; const uint8_t* d_dd; const float* ss_table;
+    const orc_score_params* prm; long long c0, nc; float *scores, *modscores;
+    long long ld, off;
+} orc_sm_job;
+
+static void* orc_sm_thread(void* arg)
+{
+    orc_sm_job* j = (orc_sm_job*)arg;
+    orc_score_matrix(j->Lq, j->q_tf, j->q_bkg, j->q_ss, j->q_dd, j->N, j->P, j->d_tf, j->d_bkg,
+                     j->d_pro, j->d_ss, j->d_dd, j->ss_table, j->prm, j->c0, j->nc,
+                     j->scores + j->off, j->modscores + j->off, j->ld);
+    return NULL;
+}
+
+void orc_score_matrix_mt(int nthreads, int Lq, const float* q_tf, const float* q_bkg,
+                         const float* q_ss, const uint8_t* q_dd,
+                         long long N, int P, const float* d_tf, const float* d_bkg,
+                         const int32_t* d_pro, const float* d_ss, const uint8_t* d_dd,
+                         const float* ss_table, const orc_score_params* prm,
+                         long long col0, long long ncols,
+                         float* scores, float* modscores, long long ld)
+{
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    orc_sm_job jobs[256];
+    long long per = (ncols + nthreads - 1) / nthreads;
+    int nt = 0;
+    for (int t = 0; t < nthreads; t++) {
+        long long a = (long long)t * per, b = a + per;
+        if (b > ncols) b = ncols;
+        if (a >= b) break;
+        orc_sm_job j = {Lq, q_tf, q_bkg, q_ss, q_dd, N, P, d_tf, d_bkg, d_pro, d_ss, d_dd,
+                        ss_table, prm, col0 + a, b - a, scores, modscores, ld, a};
+        jobs[nt] = j;
+        pthread_create(&th[nt], NULL, orc_sm_thread, &jobs[nt]);
+        nt++;
+    }
+    for (int t = 0; t < nt; t++) pthread_join(th[t], NULL);
+}

@@ -1,0 +1,76 @@
+/*
+ * CPU oracle for the COTHER search path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A single-threaded plain-C restatement of the reference's GPU kernels
+ * (the reference has no CPU path of its own). Only the tests, the smoke
+ * check and the benchmark's CPU-baseline leg may load it, and only as the
+ * checker; the product library never links it.
+ *
+ * Every function cites the reference file:line it follows. Arithmetic is
+ * FP32 in the reference's operation order; multiply-adds that the reference
+ * compiler contracts are written as fmaf(), and the file is compiled with
+ * -ffp-contract=off so no other contraction happens.
+ */
+#ifndef COTHER_ORACLE_H
+#define COTHER_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* distance-list byte layout shared by the oracle's inputs:
+ * [0] = number of distances, [1..99] = distances, 255 = no data */
+#define ORC_NDSTSLOTS 100
+#define ORC_NOTABLE_SS 30
+
+typedef struct orc_score_params {
+    float ssswgt;     /* SSSWGT */
+    float ddmswgt;    /* DDMSWGT */
+    int   dstsegm;    /* DSTSEGM */
+    float initshift;  /* 0.002 with MAPALN=1, 0.0003 otherwise */
+} orc_score_params;
+
+/* natural logarithm restated from its series (see oracle.c) */
+float orc_logf(float x);
+
+/* DDMS score table entry for two raw distances (255 = no data) */
+float orc_dms_pair_score(int d1, int d2);
+
+/* DDMS between two distance lists (uint8, slot 0 = count); returns the
+ * weighted, transformed score; *rawsum receives the top-3 segment sum;
+ * *computed is 0 when a list is shorter than dstsegm */
+float orc_ddms_cell(const uint8_t* qlist, const uint8_t* dlist, int dstsegm,
+                    float ddmswgt, float* rawsum, int* computed);
+
+/* Score matrices for one query against N database positions.
+ *   q_tf [20][Lq], q_bkg [20], q_ss [3][Lq], q_dd [Lq][100] (uint8)
+ *   d_tf [20][N], d_bkg [20][P], d_pro [N], d_ss [3][N], d_dd [N][100]
+ *   ss_table [30][30]
+ *   out scores / modscores: [Lq][ld] (columns [col0, col0+ncols))
+ * Columns col0..col0+ncols-1 of the database are computed. */
+void orc_score_matrix(int Lq, const float* q_tf, const float* q_bkg, const float* q_ss,
+                      const uint8_t* q_dd,
+                      long long N, int P, const float* d_tf, const float* d_bkg,
+                      const int32_t* d_pro, const float* d_ss, const uint8_t* d_dd,
+                      const float* ss_table, const orc_score_params* prm,
+                      long long col0, long long ncols,
+                      float* scores, float* modscores, long long ld);
+
+/* Multi-threaded wrapper over orc_score_matrix (columns split across
+ * nthreads host threads). */
+void orc_score_matrix_mt(int nthreads, int Lq, const float* q_tf, const float* q_bkg,
+                         const float* q_ss, const uint8_t* q_dd,
+                         long long N, int P, const float* d_tf, const float* d_bkg,
+                         const int32_t* d_pro, const float* d_ss, const uint8_t* d_dd,
+                         const float* ss_table, const orc_score_params* prm,
+                         long long col0, long long ncols,
+                         float* scores, float* modscores, long long ld);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,87 @@
+"""CPU tests of the oracle: pinned against the reference's own CPU code and
+golden vectors (no GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+
+def test_logf_accuracy(oracle_lib):
+    rng = np.random.default_rng(5)
+    xs = np.exp(rng.uniform(-87, 88, 20000)).astype(np.float32)
+    xs = np.concatenate([xs, np.float32([1e-40, 1e-45, 1.0, 2.0, 0.5, 3.4e38, 1.4142135, 0.70710677])])
+    got = np.array([oracle_lib.logf(float(x)) for x in xs], np.float64)
+    ref = np.log(xs.astype(np.float64))
+    ulp = np.abs(got - ref) / np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64)
+    ulp[ref == 0] = np.abs(got[ref == 0]) / np.spacing(np.float32(1))
+    assert ulp.max() < 2.0
+
+
+def test_dms_pair_scores(oracle_lib):
+    L = oracle_lib.lib()
+    # table values of the two-level interpolation: s(d1,d2) = 0.35 + 0.02*min - 0.0375*max
+    for d1 in range(0, 25):
+        for d2 in range(0, 25):
+            a, b = min(max(d1, d2), 20), min(min(d1, d2), 20)
+            want = 0.35 + 0.02 * b - 0.0375 * a
+            assert abs(L.orc_dms_pair_score(d1, d2) - want) < 1e-6
+    assert L.orc_dms_pair_score(255, 3) == -1.0
+    assert L.orc_dms_pair_score(7, 255) == -1.0
+
+
+def test_ddms_matches_reference_cpu_code(oracle_lib):
+    """The oracle's DDMS segment DP equals the reference's own CPU
+    restatement (cother-scores-optimizer/ddms.cxx) on committed vectors."""
+    z = np.load(os.path.join(GOLDEN, "ddms_ref.npz"))
+    n = 0
+    for q, d, r in zip(z["qlists"], z["dlists"], z["ref"]):
+        s, raw, comp = oracle_lib.ddms_cell(q, d)
+        if r == -777.0:
+            continue
+        assert comp == 1
+        assert np.float32(np.rint(np.float32(raw) * np.float32(16.0))) == r
+        n += 1
+    assert n > 300
+
+
+def test_ddms_matches_reference_live(oracle_lib):
+    """Same check against the reference library built here, when present."""
+    R = oracle_lib.ref_lib()
+    if R is None:
+        pytest.skip("reference tree not available")
+    from cother_b200 import synth
+    q = synth.make_profiles([70], 1234, True)
+    d = synth.make_profiles([90, 30], 1235, False)
+    ql, dl = q.dd_lists(), d.dd_lists()
+    for i in range(0, 70, 3):
+        for j in range(0, 120, 7):
+            s, raw, comp = oracle_lib.ddms_cell(ql[i], dl[j])
+            x = np.full(110, 255, np.int32); x[:ql[i][0] + 1] = ql[i][:ql[i][0] + 1]
+            y = np.full(110, 255, np.int32); y[:dl[j][0] + 1] = dl[j][:dl[j][0] + 1]
+            r = R.ref_ddms_scaled_sum(x.ctypes.data, y.ctypes.data)
+            if r == -777.0:
+                continue
+            assert np.float32(np.rint(np.float32(raw) * np.float32(16.0))) == r
+
+
+def test_ddms_short_lists(oracle_lib):
+    q = np.full(100, 255, np.uint8); q[0] = 5; q[1:6] = [5, 6, 7, 8, 9]
+    d = np.full(100, 255, np.uint8); d[0] = 40; d[1:41] = 8
+    s, raw, comp = oracle_lib.ddms_cell(q, d, dstsegm=6)
+    assert comp == 0 and s == 0.0
+    q[0] = 6; q[6] = 10
+    s, raw, comp = oracle_lib.ddms_cell(q, d, dstsegm=6)
+    assert comp == 1
+
+
+def test_score_matrix_oracle_shapes(oracle_lib, ss_table):
+    from cother_b200 import synth
+    q = synth.make_profiles([23], 3, True)
+    db = synth.make_profiles([17, 40, 5], 4, False)
+    sc, ms = oracle_lib.score_matrix(q, db, ss_table)
+    assert sc.shape == (23, 62) and ms.shape == (23, 62)
+    assert np.isfinite(sc).all() and np.isfinite(ms).all()
+    sc2, ms2 = oracle_lib.score_matrix(q, db, ss_table, col0=17, ncols=40, nthreads=3)
+    assert np.array_equal(sc2, sc[:, 17:57]) and np.array_equal(ms2, ms[:, 17:57])

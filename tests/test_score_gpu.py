@@ -1,0 +1,83 @@
+"""Score matrix on the GPU vs the CPU oracle: bit-identical cells."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(q, db, ss_table, max_slab=0, **opt):
+    import cother_b200 as cb
+    o = cb.Options.defaults()
+    for k, v in opt.items():
+        setattr(o, k, v)
+    with cb.BatchProcessing(ss_table, o) as bp:
+        if max_slab:
+            bp.set_max_slab_positions(max_slab)
+        bp.transfer_cpm_data(db)
+        bp.process_score_matrix(q)
+        sc, ms, first = bp.read_score_matrix(q.npositions, db.npositions)
+    return sc, ms, first
+
+
+def test_score_matrix_bit_exact_small(oracle_lib, ss_table):
+    from cother_b200 import synth
+    q = synth.make_profiles([37], 21, True)
+    db = synth.make_profiles([45, 3, 120, 64, 31], 22, False)
+    sc, ms, first = _run(q, db, ss_table)
+    assert first == 0
+    osc, oms = oracle_lib.score_matrix(q, db, ss_table, nthreads=8)
+    assert sc.shape == osc.shape
+    assert np.array_equal(sc, osc), np.abs(sc - osc).max()
+    assert np.array_equal(ms, oms), np.abs(ms - oms).max()
+
+
+def test_score_matrix_bit_exact_workload(oracle_lib, ss_table):
+    from cother_b200 import synth
+    q, db = synth.make_workload("q200_db1k", seed=3, ndb=60)
+    sc, ms, _ = _run(q, db, ss_table)
+    osc, oms = oracle_lib.score_matrix(q, db, ss_table, nthreads=16)
+    assert np.array_equal(sc, osc)
+    assert np.array_equal(ms, oms)
+
+
+def test_score_matrix_last_slab(oracle_lib, ss_table):
+    """Multi-slab processing: the last slab holds the trailing profiles."""
+    from cother_b200 import synth
+    q = synth.make_profiles([50], 31, True)
+    lens = [70, 20, 90, 33, 64, 12]
+    db = synth.make_profiles(lens, 32, False)
+    sc, ms, first = _run(q, db, ss_table, max_slab=100)
+    # slabs of <=100 positions: [70,20] [90] [33,64] [12]
+    assert first == 5
+    col0 = sum(lens[:5])
+    osc, oms = oracle_lib.score_matrix(q, db, ss_table, col0=col0, ncols=12)
+    assert np.array_equal(sc, osc) and np.array_equal(ms, oms)
+
+
+def test_score_matrix_options(oracle_lib, ss_table):
+    """DDMS off, other weights, DSTSEGM and MAPALN=0 shift."""
+    from cother_b200 import synth
+    q = synth.make_profiles([21], 41, True)
+    db = synth.make_profiles([33, 18], 42, False)
+    for opt, orc in [
+        (dict(ddmswgt=0.0), dict(ddmswgt=0.0)),
+        (dict(ssswgt=0.3, ddmswgt=0.5, dstsegm=3), dict(ssswgt=0.3, ddmswgt=0.5, dstsegm=3)),
+        (dict(mapaln=0), dict(initshift=0.0003)),
+    ]:
+        sc, ms, _ = _run(q, db, ss_table, **opt)
+        osc, oms = oracle_lib.score_matrix(q, db, ss_table, **orc)
+        assert np.array_equal(sc, osc), opt
+        assert np.array_equal(ms, oms), opt
+
+
+def test_bad_inputs_fail_loudly(ss_table):
+    import cother_b200 as cb
+    from cother_b200 import synth
+    q = synth.make_profiles([10], 5, True)
+    with cb.BatchProcessing(ss_table) as bp:
+        with pytest.raises(cb.CbpError):
+            bp.process_score_matrix(q)  # no database chunk yet
+        db = synth.make_profiles([12], 6, False)
+        db.dd[0, 3] = 150.0  # distance count beyond 99
+        with pytest.raises(cb.CbpError):
+            bp.transfer_cpm_data(db)
