@@ -75,8 +75,14 @@ def load_library(path: str | None = None):
         "cbp_wait_idle": (i32, [vp]),
         "cbp_read_score_matrix": (i32, [vp, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
         "cbp_set_max_slab_positions": (i32, [vp, sz]),
+        "cbp_read_phase1": (i32, [vp, vp, vp, vp, vp, vp, sz, ctypes.POINTER(sz), vp,
+                                  ctypes.POINTER(sz)]),
+        "cbp_read_btck": (i32, [vp, vp, sz]),
+        "cbp_score_threshold": (None, [sz, ctypes.c_uint64, f32, f32, f32, ctypes.POINTER(f32),
+                                       ctypes.POINTER(f32)]),
         "cbp_stage_times": (i32, [vp, vp, i32]),
         "cbp_launch_count": (i32, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "cbp_stage_launches": (i32, [vp, vp, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -84,6 +90,22 @@ def load_library(path: str | None = None):
         fn.argtypes = args
     _lib = L
     return L
+
+
+# gapped Karlin-Altschul parameters of the reference's statistical
+# configuration (src/env/cother.par, section [GAPPED_A_1])
+GAPPED_LAMBDA = 0.561132
+GAPPED_K = 0.001488
+
+
+def score_threshold(query_len: int, db_len: int, evalue: float = 10.0,
+                    lam: float = GAPPED_LAMBDA, K: float = GAPPED_K):
+    """(score threshold, log E-value threshold) as the reference's job
+    dispatcher derives them (cbp_score_threshold)."""
+    a, b = ctypes.c_float(), ctypes.c_float()
+    load_library().cbp_score_threshold(int(query_len), int(db_len), float(evalue), float(lam),
+                                       float(K), ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
 
 
 def _check(rc: int) -> None:
@@ -172,10 +194,39 @@ class BatchProcessing:
         n = ncols.value
         return sc[:, :n], ms[:, :n], first.value
 
+    def read_phase1(self):
+        """Phase-1 records of the last slab: dict of arrays (score, psts,
+        beg, end, passed) and the pass list."""
+        n = self._db.nprofiles if self._db is not None else 0
+        score = np.zeros(n, np.float32)
+        psts = np.zeros(n, np.float32)
+        beg = np.zeros(n, np.uint32)
+        end = np.zeros(n, np.uint32)
+        passed = np.zeros(n, np.int32)
+        plist = np.zeros(n, np.int32)
+        nprof, npass = ctypes.c_size_t(), ctypes.c_size_t()
+        _check(load_library().cbp_read_phase1(self._h, score.ctypes.data, psts.ctypes.data,
+                                               beg.ctypes.data, end.ctypes.data, passed.ctypes.data,
+                                               n, ctypes.byref(nprof), plist.ctypes.data,
+                                               ctypes.byref(npass)))
+        k = nprof.value
+        return ({"score": score[:k], "psts": psts[:k], "beg": beg[:k], "end": end[:k],
+                 "passed": passed[:k]}, plist[:npass.value])
+
+    def read_btck(self, nrows: int, max_cols: int):
+        b = np.zeros((nrows, max_cols), np.uint8)
+        _check(load_library().cbp_read_btck(self._h, b.ctypes.data, max_cols))
+        return b
+
     def stage_times(self) -> list:
         buf = (ctypes.c_float * 6)()
         n = load_library().cbp_stage_times(self._h, buf, 6)
         return [buf[i] for i in range(n)]
+
+    def stage_launches(self) -> list:
+        buf = (ctypes.c_uint64 * 6)()
+        n = load_library().cbp_stage_launches(self._h, buf, 6)
+        return [int(buf[i]) for i in range(n)]
 
     def launch_count(self) -> int:
         v = ctypes.c_uint64()

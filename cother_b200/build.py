@@ -29,11 +29,14 @@ LIB_SYNTH = os.path.join(HERE, "libcbsynth.so")
 CUDA_SOURCES = [
     "api.cu",
     "score_kernel.cu",
+    "dp1_kernel.cu",
 ]
 CUDA_HEADERS = [
     "common.cuh",
     "cbmath.cuh",
     "layout.h",
+    "score_kernel.cuh",
+    "dp1_kernel.cuh",
 ]
 
 

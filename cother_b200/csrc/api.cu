@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "layout.h"
 #include "score_kernel.cuh"
+#include "dp1_kernel.cuh"
 
 namespace cbp {
 
@@ -82,17 +83,20 @@ struct cbp_context {
     float score_thld = 0.f;
     float logE_thld = 0.f;
     // working buffers
-    DevBuf scores, modscores;
+    DevBuf scores, modscores, btck, bandbuf, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
     // last slab
     long long last_col0 = 0;
     int last_ncols = 0;
     long long last_ld = 0;
     int last_first_profile = 0;
     int last_Lq = 0;
+    int last_nprof = 0;
+    int last_npass = 0;
     // instrumentation
     cudaEvent_t ev[8]{};
     float stage_ms[6] = {0, 0, 0, 0, 0, 0};
     uint64_t launches = 0;
+    uint64_t stage_launches[6] = {0, 0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -251,8 +255,9 @@ std::vector<Slab> plan_slabs(const cbp_context* c, int Lq)
 {
     const ProfilesStore& db = c->db;
     const int P = (int)db.h_plen.size();
-    // bytes per slab position: scores + modscores per query position
-    const size_t per_pos = (size_t)Lq * 8 + 64;
+    // bytes per slab position: scores + modscores + backtrack byte per query
+    // position, the DP band strip and per-profile records
+    const size_t per_pos = (size_t)Lq * 9 + 5 * 4 + 64;
     size_t cap = c->mem_budget / per_pos;
     if (c->max_slab_positions) cap = std::min(cap, c->max_slab_positions);
     cap = std::min<size_t>(cap, (size_t)1 << 30);
@@ -343,8 +348,9 @@ int cbp_destroy(cbp_context* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->db.release();
     c->query.release();
-    c->scores.release();
-    c->modscores.release();
+    for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax, &c->dpcoords,
+                      &c->dprecs, &c->passidx, &c->passdst, &c->passcnt})
+        b->release();
     c->sstab.release();
     c->dmstab.release();
     for (auto& e : c->ev)
@@ -401,12 +407,24 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         if ((size_t)Lq != query_len) throw Error(CBP_ERR_ARG, "query_len differs from the query profile length");
         c->launches = 0;
         for (float& m : c->stage_ms) m = 0.f;
+        for (uint64_t& m : c->stage_launches) m = 0;
 
         std::vector<Slab> slabs = plan_slabs(c, Lq);
-        size_t maxcols = 0;
-        for (const Slab& s : slabs) maxcols = std::max(maxcols, (size_t)align_up(s.ncols, 32));
+        size_t maxcols = 0, maxprof = 0;
+        for (const Slab& s : slabs) {
+            maxcols = std::max(maxcols, (size_t)align_up(s.ncols, 32));
+            maxprof = std::max(maxprof, (size_t)(s.p1 - s.p0));
+        }
         c->scores.reserve((size_t)Lq * maxcols * sizeof(float));
         c->modscores.reserve((size_t)Lq * maxcols * sizeof(float));
+        c->btck.reserve((size_t)Lq * maxcols);
+        c->bandbuf.reserve(5 * maxcols * sizeof(float));
+        c->dpmax.reserve(maxprof * sizeof(float));
+        c->dpcoords.reserve(maxprof * sizeof(uint32_t));
+        c->dprecs.reserve(maxprof * sizeof(Dp1Rec));
+        c->passidx.reserve(maxprof * sizeof(int));
+        c->passdst.reserve(maxprof * sizeof(long long));
+        c->passcnt.reserve(64);
 
         for (const Slab& s : slabs) {
             ScoreArgs a;
@@ -425,19 +443,52 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             a.dmstab = c->dmstab.as<float>();
             a.scores = c->scores.as<float>();
             a.modscores = c->modscores.as<float>();
+
+            Dp1Args d;
+            d.scores = a.scores;
+            d.ld = a.ld;
+            d.Lq = Lq;
+            d.qtrn = c->query.view.trn;
+            d.db = c->db.view;
+            d.col0 = s.col0;
+            d.p0 = s.p0;
+            d.nprof = s.p1 - s.p0;
+            d.btck = c->btck.as<uint8_t>();
+            d.bandbuf = c->bandbuf.as<float>();
+            d.maxsc = c->dpmax.as<float>();
+            d.maxcoords = c->dpcoords.as<uint32_t>();
+            d.recs = c->dprecs.as<Dp1Rec>();
+
             CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
             launch_score_matrix(a, c->stream);
-            c->launches++;
             CBP_CUDA(cudaEventRecord(c->ev[1], c->stream));
-            CBP_CUDA(cudaEventSynchronize(c->ev[1]));
+            launch_dp1(d, c->stream);
+            CBP_CUDA(cudaEventRecord(c->ev[2], c->stream));
+            launch_dp1_finalize(d, c->score_thld, c->stream);
+            launch_pass_compact(d, c->passidx.as<int>(), c->passdst.as<long long>(), c->passcnt.as<int>(),
+                                reinterpret_cast<long long*>(c->passcnt.as<char>() + 8), c->stream);
+            CBP_CUDA(cudaEventRecord(c->ev[3], c->stream));
+            c->launches += 4;
+            c->stage_launches[0] += 1;
+            c->stage_launches[1] += 1;
+            c->stage_launches[2] += 2;
+            int npass = 0;
+            CBP_CUDA(cudaMemcpyAsync(&npass, c->passcnt.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CBP_CUDA(cudaStreamSynchronize(c->stream));
             float ms = 0.f;
             CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
             c->stage_ms[0] += ms;
+            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]));
+            c->stage_ms[1] += ms;
+            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+            c->stage_ms[2] += ms;
             c->last_col0 = s.col0;
             c->last_ncols = s.ncols;
             c->last_ld = a.ld;
             c->last_first_profile = s.p0;
             c->last_Lq = Lq;
+            c->last_nprof = d.nprof;
+            c->last_npass = npass;
         }
         CBP_CUDA(cudaStreamSynchronize(c->stream));
     });
@@ -467,11 +518,74 @@ int cbp_read_score_matrix(cbp_context* c, float* scores, float* modscores, size_
     });
 }
 
+int cbp_read_phase1(cbp_context* c, float* score, float* psts, uint32_t* beg, uint32_t* end,
+                    int* passed, size_t nmax, size_t* nprof, int* pass_list, size_t* npass)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!c->last_Lq) throw Error(CBP_ERR_STATE, "no processed query");
+        const size_t n = (size_t)c->last_nprof;
+        if (nprof) *nprof = n;
+        if (npass) *npass = (size_t)c->last_npass;
+        if (nmax < n) throw Error(CBP_ERR_ARG, "output arrays too small");
+        std::vector<Dp1Rec> r(n);
+        CBP_CUDA(cudaMemcpy(r.data(), c->dprecs.p, n * sizeof(Dp1Rec), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; i++) {
+            if (score) score[i] = r[i].score;
+            if (psts) psts[i] = r[i].psts;
+            if (beg) beg[i] = r[i].beg;
+            if (end) end[i] = r[i].end;
+            if (passed) passed[i] = r[i].passed;
+        }
+        if (pass_list && c->last_npass > 0)
+            CBP_CUDA(cudaMemcpy(pass_list, c->passidx.p, (size_t)c->last_npass * sizeof(int),
+                                cudaMemcpyDeviceToHost));
+    });
+}
+
+int cbp_read_btck(cbp_context* c, uint8_t* btck, size_t ld)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!c->last_Lq) throw Error(CBP_ERR_STATE, "no processed query");
+        if (ld < (size_t)c->last_ncols) throw Error(CBP_ERR_ARG, "ld smaller than the slab width");
+        CBP_CUDA(cudaMemcpy2D(btck, ld, c->btck.p, c->last_ld, (size_t)c->last_ncols, c->last_Lq,
+                              cudaMemcpyDeviceToHost));
+    });
+}
+
+void cbp_score_threshold(size_t query_len, uint64_t db_len, float evalue, float gapped_lambda,
+                         float gapped_k, float* score_threshold, float* log_evalue_threshold)
+{
+    const size_t sspace = query_len * (size_t)db_len;
+    float ev = evalue;
+    float sthld = 999.0f, lthld = -99.0f;
+    if (ev > 0.0f && sspace > 0 && gapped_lambda > 0.0f && gapped_k > 0.0f) {
+        lthld = logf(ev);
+        ev = ev < 1.0f ? ev * 10.0f : ev * 3.0f;
+        ev /= gapped_k * (float)sspace;
+        if (ev > 0.0f) {
+            float sc = -logf(ev) / gapped_lambda;
+            sthld = sc < 0.0f ? 0.0f : sc;
+        }
+    }
+    if (score_threshold) *score_threshold = sthld;
+    if (log_evalue_threshold) *log_evalue_threshold = lthld;
+}
+
 int cbp_stage_times(cbp_context* c, float* ms, int n)
 {
     if (!c || !ms) return 0;
     int k = std::min(n, 6);
     for (int i = 0; i < k; i++) ms[i] = c->stage_ms[i];
+    return k;
+}
+
+int cbp_stage_launches(cbp_context* c, uint64_t* launches, int n)
+{
+    if (!c || !launches) return 0;
+    int k = std::min(n, 6);
+    for (int i = 0; i < k; i++) launches[i] = c->stage_launches[i];
     return k;
 }
 

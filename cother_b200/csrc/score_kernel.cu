@@ -61,6 +61,21 @@ __device__ __forceinline__ void register_max(float (&ms)[3], uint32_t (&mc)[3], 
     }
 }
 
+// Saturating add/multiply: the result clamped to [0, 1] in one FMA-pipe
+// instruction.
+__device__ __forceinline__ float sat_add(float a, float b)
+{
+    float r;
+    asm("add.sat.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float sat_mul(float a, float b)
+{
+    float r;
+    asm("mul.sat.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
 // One diagonal of the DDMS segment DP. Elements e = 0,1,... pair query list
 // element oq+e with database list element od+e (upper diagonals: oq = 0,
 // od = j; lower: oq = i, od = 0). Pair scores at even offsets within each
@@ -69,62 +84,79 @@ __device__ __forceinline__ void register_max(float (&ms)[3], uint32_t (&mc)[3], 
 // restarts when the running sum has fallen to zero, and the best segment of
 // length >= DSTSEGM ending in each 4-step is offered to the top-3 register
 // (ddms2s_h2.cuh:124-176, 288-396).
+//
+// The pair scores come pre-scaled by 2^-7, so every running sum stays in
+// [0, 1) and max(sum, 0) is one saturating add; scaling by a power of two
+// commutes exactly with IEEE rounding, so the sums are the reference's
+// times 2^-7, bit for bit. The segment length is a small exact float:
+// len_k = len_{k-1} * [sum_{k-1} > 0] + 1, the indicator being
+// sat(sum * 2^100) (every positive sum here is far above 2^-100). A step's
+// candidate is max_k sum_k * [len_k >= DSTSEGM] and sits at the first k that
+// attains it, which is the reference's strict "<" scan.
 __device__ __forceinline__ void ddms_diagonal(
     const uint8_t* __restrict__ q, const uint8_t* __restrict__ d,
-    const float* __restrict__ T, int lim, int oq, int od, int segm1,
+    const float* __restrict__ T, int lim, int oq, int od, float nsegm1,
     float (&ms)[3], uint32_t (&mc)[3])
 {
+    constexpr float kBig = 0x1p100f;
     float s0 = T[q[0] * kDstCard + d[0]];
-    float segsco = hmax(s0, 0.0f);
-    int segb = 0;
+    float t = sat_add(s0, 0.0f);
+    float ls = 1.0f;
     const uint32_t cbase = ((uint32_t)oq << 24) | ((uint32_t)oq << 16) | ((uint32_t)od << 8) | (uint32_t)od;
     for (int x = 0; x < lim; x += 4) {
         const float s2 = T[q[x + 2] * kDstCard + d[x + 2]];
         const float s4 = T[q[x + 4] * kDstCard + d[x + 4]];
         const float s1 = 0.5f * (s0 + s2);
         const float s3 = 0.5f * (s2 + s4);
-        float scom = 0.0f;
-        int bb = 0, be = 0;
-#define CBP_DDMS_UPD(S, K)                                             \
-        {                                                              \
-            const int e = x + (K);                                     \
-            if (segsco == 0.0f) segb = e;                              \
-            segsco = hmax(segsco + (S), 0.0f);                         \
-            if (scom < segsco && segb + segm1 <= e) {                  \
-                scom = segsco; bb = segb; be = e;                      \
-            }                                                          \
-        }
-        CBP_DDMS_UPD(s1, 1)
-        CBP_DDMS_UPD(s2, 2)
-        CBP_DDMS_UPD(s3, 3)
-        CBP_DDMS_UPD(s4, 4)
-#undef CBP_DDMS_UPD
+        const float l1 = __fmaf_rn(ls, sat_mul(t, kBig), 1.0f);
+        const float t1 = sat_add(t, s1);
+        const float l2 = __fmaf_rn(l1, sat_mul(t1, kBig), 1.0f);
+        const float t2 = sat_add(t1, s2);
+        const float l3 = __fmaf_rn(l2, sat_mul(t2, kBig), 1.0f);
+        const float t3 = sat_add(t2, s3);
+        const float l4 = __fmaf_rn(l3, sat_mul(t3, kBig), 1.0f);
+        const float t4 = sat_add(t3, s4);
+        const float v1 = t1 * sat_add(l1, nsegm1);
+        const float v2 = t2 * sat_add(l2, nsegm1);
+        const float v3 = t3 * sat_add(l3, nsegm1);
+        const float v4 = t4 * sat_add(l4, nsegm1);
+        const float scom = fmaxf(fmaxf(v1, v2), fmaxf(v3, v4));
         if (scom != 0.0f) {
-            const uint32_t c = cbase + (((uint32_t)bb << 24) | ((uint32_t)be << 16) |
-                                        ((uint32_t)bb << 8) | (uint32_t)be);
+            int k;
+            float lk;
+            if (v1 == scom) { k = 1; lk = l1; }
+            else if (v2 == scom) { k = 2; lk = l2; }
+            else if (v3 == scom) { k = 3; lk = l3; }
+            else { k = 4; lk = l4; }
+            const uint32_t be = (uint32_t)(x + k);
+            const uint32_t bb = be + 1u - (uint32_t)lk;
+            const uint32_t c = cbase + ((bb << 24) | (be << 16) | (bb << 8) | be);
             register_max(ms, mc, scom, c);
         }
         s0 = s4;
+        t = t4;
+        ls = l4;
     }
 }
 
 // DDMS of one cell (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:433-500).
+// Returns the top-3 sum in the reference's scale.
 __device__ __forceinline__ float ddms_cell(const uint8_t* __restrict__ q, int len1,
                                            const uint8_t* __restrict__ d, int len2,
                                            const float* __restrict__ T, int dstsegm)
 {
     float ms[3] = {0.0f, 0.0f, 0.0f};
     uint32_t mc[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
-    const int segm1 = dstsegm - 1;
+    const float nsegm1 = -(float)(dstsegm - 1);
     for (int j = len2 >> 2; 0 <= j; j -= 2)
-        ddms_diagonal(q, d + j, T, min(len1, len2 - j), 0, j, segm1, ms, mc);
+        ddms_diagonal(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mc);
     for (int i = len1 >> 2; 0 < i; i -= 2)
-        ddms_diagonal(q + i, d, T, min(len2, len1 - i), i, 0, segm1, ms, mc);
+        ddms_diagonal(q + i, d, T, min(len2, len1 - i), i, 0, nsegm1, ms, mc);
     float sum = 0.0f;
     sum = sum + ms[0];
     sum = sum + ms[1];
     sum = sum + ms[2];
-    return sum;
+    return sum * 128.0f;
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -150,7 +182,7 @@ score_matrix_kernel(const ScoreArgs a)
     const int rowb = blockIdx.y * kRows;
     const long long N = a.db.N;
 
-    for (int i = tid; i < kDstCard * kDstCard; i += kThreads) s_dms[i] = a.dmstab[i];
+    for (int i = tid; i < kDstCard * kDstCard; i += kThreads) s_dms[i] = a.dmstab[i] * 0x1p-7f;
     for (int i = tid; i < kSSCard * kSSCard; i += kThreads) s_sst[i] = a.sstab[i];
 
     // database columns of this block

@@ -90,6 +90,44 @@ def make_profiles(lens, seed: int, predicted: bool, window: int = 64,
                       names=[f"synth{seed}_{i}" for i in range(P)])
 
 
+def plant_homologs(query: ProfileSet, db: ProfileSet, fraction: float, seed: int,
+                   noise: float = 0.3) -> np.ndarray:
+    """Overwrite a seeded subset of database profiles with noisy copies of
+    query segments (target frequencies, SS probabilities, transitions and
+    distance lists), so that a search finds true hits. Returns the indices of
+    the planted profiles."""
+    rng = np.random.default_rng(seed)
+    P = db.nprofiles
+    k = int(round(fraction * P))
+    if k <= 0:
+        return np.zeros(0, np.int64)
+    picks = np.sort(rng.choice(P, size=k, replace=False))
+    Lq = query.npositions
+    starts = db.starts
+    for p in picks:
+        Ld = int(db.lens[p])
+        n = int(min(Ld, Lq) * rng.uniform(0.5, 1.0))
+        if n < 8:
+            continue
+        qa = int(rng.integers(0, Lq - n + 1))
+        da = int(rng.integers(0, Ld - n + 1))
+        s0 = int(starts[p]) + da
+        w = 1.0 - noise
+        db.tf[:, s0:s0 + n] = (w * query.tf[:, qa:qa + n] + noise * db.tf[:, s0:s0 + n])
+        db.ss[:, s0:s0 + n] = (w * query.ss[:, qa:qa + n] + noise * db.ss[:, s0:s0 + n])
+        t0 = int(starts[p]) + int(p) + 1 + da
+        db.trn[:, t0:t0 + n] = query.trn[:, qa + 1:qa + 1 + n]
+        dl = query.dd[:, qa:qa + n].copy()
+        jitter = rng.integers(-1, 2, size=dl[1:].shape)
+        vals = dl[1:]
+        keep = vals != 255.0
+        vals[keep] = np.clip(vals[keep] + jitter[keep], 0, 64)
+        db.dd[:, s0:s0 + n] = dl
+        db.aa[s0:s0 + n] = query.aa[qa:qa + n]
+        db.ssstate[s0:s0 + n] = query.ssstate[qa:qa + n]
+    return picks
+
+
 def lognormal_lengths(n: int, median: float, lo: int, hi: int, seed: int,
                       sigma: float = 0.5) -> np.ndarray:
     rng = np.random.default_rng(seed)
@@ -125,11 +163,18 @@ def db_lengths(name: str, seed: int = 7, ndb: int | None = None) -> np.ndarray:
     return uniform_lengths(n, law[1], law[2], seed)
 
 
-def make_workload(name: str, seed: int = 7, ndb: int | None = None, qindex: int = 0):
-    """(query ProfileSet, database ProfileSet) for a named workload."""
+HOMOLOG_FRACTION = 0.01
+
+
+def make_workload(name: str, seed: int = 7, ndb: int | None = None, qindex: int = 0,
+                  homologs: float = HOMOLOG_FRACTION):
+    """(query ProfileSet, database ProfileSet) for a named workload; a
+    fraction `homologs` of the database profiles are planted homologs of
+    the query."""
     w = WORKLOADS[name]
     lens = db_lengths(name, seed, ndb)
     db = make_profiles(lens, seed=seed * 1000 + 1, predicted=False, window=w["window"])
     q = make_profiles([w["qlens"][qindex]], seed=seed * 1000 + 2 + qindex, predicted=True,
                       window=w["window"])
+    plant_homologs(q, db, homologs, seed=seed * 1000 + 3 + qindex)
     return q, db

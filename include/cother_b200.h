@@ -132,6 +132,29 @@ const char* cbp_last_error(void);
 int cbp_read_score_matrix(cbp_context* ctx, float* scores, float* modscores,
                           size_t ld, size_t* ncols, size_t* first_profile);
 
+/* Phase-1 results of the profiles of the last slab (index = profile within
+ * the slab): score with correlation bonus, #positive substitution scores,
+ * beginning/end coordinates packed (x << 16) | y, and whether the profile
+ * passed the score threshold; pass_list receives the slab indices of the
+ * passed profiles in ascending order (*npass entries). The records follow
+ * FinalizeDPPro (src/libmycu/cudp/CuBatchDP_final.cu:61-292). */
+int cbp_read_phase1(cbp_context* ctx, float* score, float* psts, uint32_t* beg,
+                    uint32_t* end, int* passed, size_t nmax, size_t* nprof,
+                    int* pass_list, size_t* npass);
+
+/* Backtrack codes of the last slab's phase-1 DP, btck[r * ld + c]
+ * (0 stop, 1 left, 2 up, 3 diagonal; src/libmycu/cudp/CuBatchDP_com.h:101-106). */
+int cbp_read_btck(cbp_context* ctx, uint8_t* btck, size_t ld);
+
+/* Phase-1 score threshold and log E-value threshold from the E-value
+ * threshold and the gapped Karlin-Altschul parameters (the [GAPPED_A_1]
+ * lambda and K of cother.par); search space = query_len * db_len.
+ * Replaces JobDispatcher::CalculateScoreThreshold
+ * (src/libmycu/cualn/JobDispatcher.cpp:809-860). */
+void cbp_score_threshold(size_t query_len, uint64_t db_len, float evalue,
+                         float gapped_lambda, float gapped_k,
+                         float* score_threshold, float* log_evalue_threshold);
+
 /* Limit the number of database positions processed per slab (0 = plan by
  * the memory budget). Used to exercise multi-slab processing. */
 int cbp_set_max_slab_positions(cbp_context* ctx, size_t max_positions);
@@ -141,6 +164,10 @@ int cbp_set_max_slab_positions(cbp_context* ctx, size_t max_positions);
  * finalization, [3] statistics, [4] MAP phase, [5] result assembly.
  * Returns the number of stages written (<= n). */
 int cbp_stage_times(cbp_context* ctx, float* ms, int n);
+
+/* Kernel launches of the last cbp_process() call per stage (same stage
+ * order as cbp_stage_times). Returns the number of stages written. */
+int cbp_stage_launches(cbp_context* ctx, uint64_t* launches, int n);
 
 /* Number of kernel launches issued by the last cbp_process() call. */
 int cbp_launch_count(cbp_context* ctx, uint64_t* launches);

@@ -340,3 +340,183 @@ void orc_score_matrix_mt(int nthreads, int Lq, const float* q_tf, const float* q
     }
     for (int t = 0; t < nt; t++) pthread_join(th[t], NULL);
 }
+
+/* ------------------------------------------------------------------------
+ * Phase-1 DP.
+ * Corner triangles (src/libmycu/cudp/CuBatchDP_init_btck.cuh:117-170): with
+ * edge = min(60, rint(0.34*max(Lq,Ld))) the cells with
+ * (Lq <= r+edge && c <= edge+r-Lq) or (Ld-edge+r <= c && r < edge) score -9
+ * (CuBatchDP_init_btck.cu:230-245). States outside the matrix are 0
+ * (DPLocInitCache, CuBatchDP_init.cuh:186-206).
+ */
+enum { ORC_MM = 0, ORC_MI, ORC_MD, ORC_IM, ORC_II, ORC_DM, ORC_DD };
+enum { ORC_STOP = 0, ORC_LEFT = 1, ORC_UP = 2, ORC_DIAG = 3 };
+
+static int orc_corner_edge(int Lq, int Ld)
+{
+    int mx = Lq > Ld ? Lq : Ld;
+    int e = (int)rintf(0.34f * (float)mx);
+    return e > 60 ? 60 : e;
+}
+
+static int orc_in_corner(int Lq, int Ld, int edge, int r, int c)
+{
+    return (Lq <= r + edge && c <= edge + r - Lq) || (Ld - edge + r <= c && r < edge);
+}
+
+float orc_dp1_profile(int Lq, int Ld, const float* S, long long lds,
+                      const float* qtrn, long long qts, const float* dtrn, long long dts,
+                      uint8_t* btck, int* maxr, int* maxc)
+{
+    const int edge = orc_corner_edge(Lq, Ld);
+    /* previous row (r-1) and current row (r) states, index c+1 (0 = boundary) */
+    size_t w = (size_t)Ld + 1;
+    float* prv = (float*)calloc(5 * w, sizeof(float));
+    float* cur = (float*)calloc(5 * w, sizeof(float));
+    float best = 0.0f;
+    int br = 0, bc = 0;
+#define PMM(a, c) a[0 * w + (c)]
+#define PMI(a, c) a[1 * w + (c)]
+#define PIM(a, c) a[2 * w + (c)]
+#define PDN(a, c) a[3 * w + (c)]
+#define PND(a, c) a[4 * w + (c)]
+    for (int r = 0; r < Lq; r++) {
+        const float qMMp = qtrn[ORC_MM * qts + r], qIMp = qtrn[ORC_IM * qts + r];
+        const float qDMp = qtrn[ORC_DM * qts + r], qMDp = qtrn[ORC_MD * qts + r];
+        const float qDDp = qtrn[ORC_DD * qts + r];
+        const float qMIc = qtrn[ORC_MI * qts + r + 1], qIIc = qtrn[ORC_II * qts + r + 1];
+        for (int k = 0; k < 5; k++) cur[k * w] = 0.0f;
+        for (int c = 0; c < Ld; c++) {
+            const float dMMp = dtrn[ORC_MM * dts + c], dIMp = dtrn[ORC_IM * dts + c];
+            const float dDMp = dtrn[ORC_DM * dts + c], dMDp = dtrn[ORC_MD * dts + c];
+            const float dDDp = dtrn[ORC_DD * dts + c];
+            const float dMIc = dtrn[ORC_MI * dts + c + 1], dIIc = dtrn[ORC_II * dts + c + 1];
+            float sc = orc_in_corner(Lq, Ld, edge, r, c) ? -9.0f : S[(size_t)r * lds + c];
+            float v1, v2, mx;
+            int b = ORC_STOP;
+            /* MM from the diagonal predecessor */
+            v1 = PMI(prv, c) + qMMp + dIMp;
+            v2 = PIM(prv, c) + qIMp + dMMp;
+            v1 = orc_hmax(v1, v2);
+            v2 = PDN(prv, c) + qDMp + dMMp;
+            v1 = orc_hmax(v1, v2);
+            v2 = PND(prv, c) + qMMp + dDMp;
+            v1 = orc_hmax(v1, v2);
+            v2 = PMM(prv, c) + qMMp + dMMp;
+            v1 = orc_hmax(v1, v2);
+            v1 = orc_hmax(v1 + sc, 0.0f);
+            mx = v1;
+            if (mx != 0.0f) b = ORC_DIAG;
+            PMM(cur, c + 1) = v1;
+            if (best < v1) { best = v1; br = r; bc = c; }
+            /* MI from above */
+            v1 = PMM(prv, c + 1) + qMMp + dMIc;
+            v2 = PMI(prv, c + 1) + qMMp + dIIc;
+            v1 = orc_hmax(v1, v2);
+            PMI(cur, c + 1) = v1;
+            if (mx < v1) { mx = v1; b = ORC_UP; }
+            /* IM from the left */
+            v1 = PMM(cur, c) + qMIc + dMMp;
+            v2 = PIM(cur, c) + qIIc + dMMp;
+            v1 = orc_hmax(v1, v2);
+            PIM(cur, c + 1) = v1;
+            if (mx < v1) { mx = v1; b = ORC_LEFT; }
+            /* DN from above */
+            v1 = PMM(prv, c + 1) + qMDp;
+            v2 = PDN(prv, c + 1) + qDDp;
+            v1 = orc_hmax(v1, v2);
+            PDN(cur, c + 1) = v1;
+            if (mx < v1) { mx = v1; b = ORC_UP; }
+            /* ND from the left */
+            v1 = PMM(cur, c) + dMDp;
+            v2 = PND(cur, c) + dDDp;
+            v1 = orc_hmax(v1, v2);
+            PND(cur, c + 1) = v1;
+            if (mx < v1) { mx = v1; b = ORC_LEFT; }
+            btck[(size_t)r * Ld + c] = (uint8_t)b;
+        }
+        float* t = prv; prv = cur; cur = t;
+    }
+#undef PMM
+#undef PMI
+#undef PIM
+#undef PDN
+#undef PND
+    free(prv);
+    free(cur);
+    *maxr = br;
+    *maxc = bc;
+    return best;
+}
+
+/* xor-butterfly warp sum (src/libmycu/cudp/CuBatchDP_final.cu:224-228):
+ * after the offsets 16,8,4,2,1 every lane holds the same value; lane 0's
+ * evaluation order is reproduced here. */
+static float orc_butterfly_sum32(const float* v)
+{
+    float a[32], b[32];
+    for (int t = 0; t < 32; t++) a[t] = v[t];
+    for (int off = 16; off >= 1; off >>= 1) {
+        for (int t = 0; t < 32; t++) b[t] = a[t] + a[t ^ off];
+        for (int t = 0; t < 32; t++) a[t] = b[t];
+    }
+    return a[0];
+}
+
+int orc_dp1_finalize(int Lq, int Ld, const float* S, long long lds, const uint8_t* btck,
+                     float maxsc, int maxr, int maxc, float thld,
+                     float* out_score, float* out_psts, uint32_t* beg, uint32_t* end)
+{
+    (void)Lq;
+    *out_score = maxsc;
+    *out_psts = 0.0f;
+    *beg = *end = 0;
+    if (maxsc <= thld) return 0;
+    float win[36];
+    for (int k = 0; k < 36; k++) win[k] = 0.0f;
+    int x = maxc, y = maxr, psts = 0, b = ORC_DIAG;
+    float sumcorr = 0.0f;
+    while (b != ORC_STOP) {
+        for (int k = 0; k < 4; k++) win[k] = win[32 + k];
+        int ndx = 4;
+        while (ndx < 36) {
+            if (x < 0 || y < 0) { b = ORC_STOP; break; }
+            b = btck[(size_t)y * Ld + x];
+            if (b == ORC_STOP) break;
+            if (b == ORC_UP) { y--; continue; }
+            if (b == ORC_LEFT) { x--; continue; }
+            win[ndx] = S[(size_t)y * lds + x];
+            if (win[ndx] > 0.0f) psts++;
+            x--; y--; ndx++;
+        }
+        float corr[32];
+        for (int t = 0; t < 32; t++)
+            corr[t] = (ndx <= t + 4) ? 0.0f
+                                     : win[t + 4] * (((win[t] + win[t + 1]) + win[t + 2]) + win[t + 3]);
+        sumcorr = sumcorr + orc_butterfly_sum32(corr);
+    }
+    sumcorr = sumcorr * 0.5f;
+    sumcorr = sumcorr < 0.0f ? -sqrtf(-sumcorr) : sqrtf(sumcorr);
+    maxsc = maxsc + sumcorr;
+    *out_score = maxsc;
+    *out_psts = (float)psts;
+    *beg = ((uint32_t)(x + 1) << 16) | (uint32_t)(y + 1);
+    *end = ((uint32_t)maxc << 16) | (uint32_t)maxr;
+    return thld < maxsc;
+}
+
+void orc_score_threshold(size_t nqyposs, size_t dbsize, float evalue, float gapped_lambda,
+                         float gapped_k, float* scorethld, float* logevthld)
+{
+    size_t sspace = nqyposs * dbsize;
+    float ev = evalue;
+    if (ev <= 0.0f) { *scorethld = 999.0f; *logevthld = -99.0f; return; }
+    *logevthld = logf(ev);
+    if (ev < 1.0f) ev *= 10.0f; else ev *= 3.0f;
+    ev /= gapped_k * (float)sspace;
+    if (ev <= 0.0f) { *scorethld = 999.0f; return; }
+    ev = logf(ev);
+    float score = -ev / gapped_lambda;
+    if (score < 0.0f) score = 0.0f;
+    *scorethld = score;
+}

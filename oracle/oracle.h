@@ -74,3 +74,38 @@ void orc_score_matrix_mt(int nthreads, int Lq, const float* q_tf, const float* q
 #endif
 
 #endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Phase-1 DP (src/libmycu/cudp/CuBatchDP_init_btck.cu:65-494) for one
+ * database profile of length Ld against a query of length Lq.
+ *   S:    scores of this profile, S[r * lds + c]
+ *   qtrn: query transitions [7][qts], entry r = into position r
+ *   dtrn: profile transitions [7][dts], pointer at the profile's beginning
+ *         vector (entry c = into position c)
+ *   btck: out [Lq][Ld] backtrack codes (0 stop, 1 left, 2 up, 3 diagonal)
+ * Returns the maximum MM score and its cell (first in row-major order
+ * among equal maxima). */
+float orc_dp1_profile(int Lq, int Ld, const float* S, long long lds,
+                      const float* qtrn, long long qts, const float* dtrn, long long dts,
+                      uint8_t* btck, int* maxr, int* maxc);
+
+/* Phase-1 finalization (src/libmycu/cudp/CuBatchDP_final.cu:61-292):
+ * backtrace from the maximum, correlation bonus, threshold.
+ * out[0] score, out[1] #positive scores; beg/end coords packed (x<<16)|y.
+ * Returns 1 if the profile passes (score > thld). */
+int orc_dp1_finalize(int Lq, int Ld, const float* S, long long lds, const uint8_t* btck,
+                     float maxsc, int maxr, int maxc, float thld,
+                     float* out_score, float* out_psts, uint32_t* beg, uint32_t* end);
+
+/* Score threshold and log E-value threshold from the E-value threshold
+ * (src/libmycu/cualn/JobDispatcher.cpp:809-860). */
+void orc_score_threshold(size_t nqyposs, size_t dbsize, float evalue, float gapped_lambda,
+                         float gapped_k, float* scorethld, float* logevthld);
+
+#ifdef __cplusplus
+}
+#endif

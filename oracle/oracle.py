@@ -55,6 +55,21 @@ def lib():
         L.orc_score_matrix.argtypes = sm_args
         L.orc_score_matrix_mt.restype = None
         L.orc_score_matrix_mt.argtypes = [ctypes.c_int] + sm_args
+        L.orc_dp1_profile.restype = ctypes.c_float
+        L.orc_dp1_profile.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
+                                      ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p,
+                                      ctypes.c_longlong, ctypes.c_void_p,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.orc_dp1_finalize.restype = ctypes.c_int
+        L.orc_dp1_finalize.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
+                                       ctypes.c_void_p, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_float, ctypes.POINTER(ctypes.c_float),
+                                       ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_uint32),
+                                       ctypes.POINTER(ctypes.c_uint32)]
+        L.orc_score_threshold.restype = None
+        L.orc_score_threshold.argtypes = [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_float,
+                                          ctypes.c_float, ctypes.c_float,
+                                          ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         _lib = L
     return _lib
 
@@ -115,3 +130,53 @@ def score_matrix(query, db, ss_table, ssswgt=0.12, ddmswgt=0.2, dstsegm=6, inits
                               d_dd.ctypes.data, T.ctypes.data, ctypes.byref(prm),
                               int(col0), int(ncols), sc.ctypes.data, ms.ctypes.data, int(ncols))
     return sc, ms
+
+
+def dp1(query, db, scores, col0, p0, nprof, thld):
+    """Phase-1 DP + finalization for profiles p0..p0+nprof-1 of db whose
+    score columns start at chunk position col0 in `scores` ([Lq][ncols]).
+
+    Returns (records, btck) with records a dict of arrays (score, psts, beg,
+    end, passed, maxsc, maxr, maxc) and btck [Lq][ncols] uint8."""
+    L = lib()
+    Lq = query.npositions
+    sc = np.ascontiguousarray(scores, np.float32)
+    ncols = sc.shape[1]
+    btck = np.zeros((Lq, ncols), np.uint8)
+    qtrn = np.ascontiguousarray(query.trn, np.float32)
+    dtrn = np.ascontiguousarray(db.trn, np.float32)
+    NT = dtrn.shape[1]
+    out = {k: [] for k in ("score", "psts", "beg", "end", "passed", "maxsc", "maxr", "maxc")}
+    starts = db.starts
+    for k in range(nprof):
+        p = p0 + k
+        Ld = int(db.lens[p])
+        c0 = int(starts[p]) - col0
+        sub = np.ascontiguousarray(sc[:, c0:c0 + Ld])
+        bt = np.zeros((Lq, Ld), np.uint8)
+        mr, mc = ctypes.c_int(), ctypes.c_int()
+        tb = int(starts[p]) + p
+        dptr = dtrn.ctypes.data + 4 * tb
+        m = L.orc_dp1_profile(Lq, Ld, sub.ctypes.data, Ld, qtrn.ctypes.data, qtrn.shape[1], dptr, NT,
+                              bt.ctypes.data, ctypes.byref(mr), ctypes.byref(mc))
+        s_, ps = ctypes.c_float(), ctypes.c_float()
+        b, e = ctypes.c_uint32(), ctypes.c_uint32()
+        pas = L.orc_dp1_finalize(Lq, Ld, sub.ctypes.data, Ld, bt.ctypes.data, m, mr.value, mc.value,
+                                 float(thld), ctypes.byref(s_), ctypes.byref(ps), ctypes.byref(b),
+                                 ctypes.byref(e))
+        btck[:, c0:c0 + Ld] = bt
+        for key, v in (("score", s_.value), ("psts", ps.value), ("beg", b.value), ("end", e.value),
+                       ("passed", pas), ("maxsc", m), ("maxr", mr.value), ("maxc", mc.value)):
+            out[key].append(v)
+    rec = {k: np.array(v) for k, v in out.items()}
+    rec["score"] = rec["score"].astype(np.float32)
+    rec["psts"] = rec["psts"].astype(np.float32)
+    rec["maxsc"] = rec["maxsc"].astype(np.float32)
+    return rec, btck
+
+
+def score_threshold(qlen, dbsize, evalue=10.0, lam=0.561132, K=0.001488):
+    a, b = ctypes.c_float(), ctypes.c_float()
+    lib().orc_score_threshold(int(qlen), int(dbsize), float(evalue), float(lam), float(K),
+                              ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
