@@ -80,6 +80,9 @@ def load_library(path: str | None = None):
         "cbp_read_btck": (i32, [vp, vp, sz]),
         "cbp_score_threshold": (None, [sz, ctypes.c_uint64, f32, f32, f32, ctypes.POINTER(f32),
                                        ctypes.POINTER(f32)]),
+        "cbp_get_hit_records": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
+        "cbp_get_search_space": (i32, [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(sz)]),
+        "cbp_set_karlin_altschul": (i32, [vp, f32, f32, f32, f32, f32, f32]),
         "cbp_stage_times": (i32, [vp, vp, i32]),
         "cbp_launch_count": (i32, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "cbp_stage_launches": (i32, [vp, vp, i32]),
@@ -106,6 +109,22 @@ def score_threshold(query_len: int, db_len: int, evalue: float = 10.0,
     load_library().cbp_score_threshold(int(query_len), int(db_len), float(evalue), float(lam),
                                        float(K), ctypes.byref(a), ctypes.byref(b))
     return a.value, b.value
+
+
+REC_FLOATS = 18
+REC_FIELDS = ["score", "org_pro_no", "pro_new_dst", "psts", "beg_coords", "end_coords",
+              "lambda_est", "K_est", "log_evalue", "log_evalue_pair", "min", "max", "expected",
+              "entropy", "lambda", "K", "identities", "gaps"]
+_REC_UINT = {"org_pro_no", "pro_new_dst", "beg_coords", "end_coords"}
+
+
+def records_table(recs: np.ndarray) -> dict:
+    """Named columns of hit records; integer fields decoded from their bits."""
+    out = {}
+    for i, name in enumerate(REC_FIELDS):
+        col = np.ascontiguousarray(recs[:, i])
+        out[name] = col.view(np.uint32).copy() if name in _REC_UINT else col.copy()
+    return out
 
 
 def _check(rc: int) -> None:
@@ -212,6 +231,28 @@ class BatchProcessing:
         k = nprof.value
         return ({"score": score[:k], "psts": psts[:k], "beg": beg[:k], "end": end[:k],
                  "passed": passed[:k]}, plist[:npass.value])
+
+    def hit_records(self) -> np.ndarray:
+        """Hit records of the last search: float32 [n][18] (CBP_REC_FLOATS);
+        use :func:`records_table` for named fields."""
+        L = load_library()
+        n = ctypes.c_size_t()
+        _check(L.cbp_get_hit_records(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, REC_FLOATS), np.float32)
+        if n.value:
+            _check(L.cbp_get_hit_records(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
+
+    def search_space(self):
+        ss, dl = ctypes.c_uint64(), ctypes.c_size_t()
+        _check(load_library().cbp_get_search_space(self._h, ctypes.byref(ss), ctypes.byref(dl)))
+        return int(ss.value), int(dl.value)
+
+    def set_karlin_altschul(self, ungapped_lambda, ungapped_k, gapped_lambda, gapped_k,
+                            gapped_alpha=0.5, gapped_beta=-1.0) -> None:
+        _check(load_library().cbp_set_karlin_altschul(self._h, ungapped_lambda, ungapped_k,
+                                                       gapped_lambda, gapped_k, gapped_alpha,
+                                                       gapped_beta))
 
     def read_btck(self, nrows: int, max_cols: int):
         b = np.zeros((nrows, max_cols), np.uint8)

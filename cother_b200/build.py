@@ -30,8 +30,10 @@ CUDA_SOURCES = [
     "api.cu",
     "score_kernel.cu",
     "dp1_kernel.cu",
+    "stats_kernel.cu",
 ]
 CUDA_HEADERS = [
+    "stats_kernel.cuh",
     "common.cuh",
     "cbmath.cuh",
     "layout.h",

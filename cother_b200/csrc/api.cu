@@ -17,6 +17,7 @@
 #include "layout.h"
 #include "score_kernel.cuh"
 #include "dp1_kernel.cuh"
+#include "stats_kernel.cuh"
 
 namespace cbp {
 
@@ -27,6 +28,78 @@ enum {
 };
 
 static thread_local std::string g_last_error;
+
+// Parameters of the significance networks and of the SS18 model
+// adjustments (the reference's static table SSE_NN_WEIGHTS_,
+// src/libmycu/cupro/CuDeviceMemory.cu:43-80): E-network mu (4x5 + 5),
+// lambda-network mu (4x5 + 5), lambda-network scale (4x5 + 5), then 9
+// adjustment parameters for each of the SS18 variants 1 and 2.
+static const float kNNWeightsTable[kNNWeights] = {
+    3.1179029f, 0.2732032f, -1.7865388f, -2.7370650f, -2.4113938f,
+    2.8802990f, -0.0845794f, 0.7335855f, -0.4155596f, -3.5943765f,
+    -2.3533863f, -0.1646748f, 2.6470928f, 1.6489798f, -0.7481717f,
+    -0.1763256f, 0.3270687f, 0.5918245f, 0.4900585f, 0.0253580f,
+    2.0547640f, 1.4051396f, -1.7874640f, 2.0048461f, 0.6947985f,
+    -0.0605839f, 0.0533123f, -1.0046299f, 0.9682557f, 0.0f,
+    -0.0173019f, -0.0051053f, 0.6215832f, -0.5038284f, 0.0f,
+    0.0600411f, -0.0527767f, 1.0036328f, -0.9667071f, 0.0f,
+    -5.9555713f, -3.1437676f, 1.8754493f, 3.4776044f, 0.0f,
+    2.8086869f, -0.5250554f, 0.3085814f, 0.5244239f, 2.4166220f,
+    -4.4935289f, -11.5416831f, 0.4601384f, 4.1707612f, 0.0f,
+    1.4710020f, 0.7746900f, 0.5248285f, -2.2621661f, 0.0f,
+    -1.4710009f, -0.7746948f, -0.5248293f, 2.2621667f, 0.0f,
+    4.8137710f, 1.0000337f, 2.0837171f, -5.3104535f, 0.0f,
+    2.5137293f, 4.2316344f, -0.8620832f, 0.8620837f, 3.1901578f,
+    0.1f, 12.0f, 1.0f, 4.0f, 0.05f, 1.0f, 0.1f, 0.35f, 0.65f,
+    0.6f, 16.0f, 1.0f, 12.0f, 0.3f, -1.7f, 0.1f, 0.45f, 0.65f,
+};
+
+// Length adjustment for edge effects and the effective search space:
+// the expected alignment length l solves l = alpha/lambda ln(K (m-l)(n-Nl))
+// + beta (Altschul et al., NAR 29, 2001), found by the bracketed iteration
+// of Gertz (2005) as in src/libpro/srcsco/AbstractScoreMatrix.cpp:303-393.
+static void length_adjustment(float lambda, float K, float alpha, float beta, size_t m,
+                              unsigned long long n, size_t N, unsigned long long* sspace_out,
+                              size_t* delta_out)
+{
+    *sspace_out = (unsigned long long)m * n;
+    *delta_out = 0;
+    if (lambda <= 0.0f || K <= 0.0f || N < 1) return;
+    const float logK = logf(K);
+    const float alratio = alpha / lambda;
+    const float max_mn = (float)(m > n ? m : n);
+    float length = 0.0f, min_length = 0.0f, max_length, nxt_length = 0.0f, sspace = 0.0f;
+    bool converged = false;
+    const float qa = (float)N;
+    const float qb = (float)(n + (unsigned long long)m * N);
+    const float qc = (float)((unsigned long long)m * n) - max_mn / K;
+    if (qc < 0.0f) return;
+    max_length = 2.0f * qc / (qb + sqrtf(qb * qb - 4.0f * qa * qc));
+    for (int j = 0; j < 20; j++) {
+        length = nxt_length;
+        sspace = ((float)m - length) * ((float)n - (float)N * length);
+        nxt_length = alratio * (logK + logf(sspace)) + beta;
+        if (length <= nxt_length) {
+            min_length = length;
+            if (nxt_length - length <= 1.0f) { converged = true; break; }
+            if (min_length == max_length) break;
+        } else {
+            max_length = length;
+        }
+        if (nxt_length < min_length || max_length < nxt_length)
+            nxt_length = (!j) ? max_length : (min_length + max_length) * 0.5f;
+    }
+    if (converged) {
+        length = ceilf(min_length);
+        if (length <= max_length) {
+            const float space2 = ((float)m - length) * ((float)n - (float)N * length);
+            nxt_length = alratio * (logK + logf(space2)) + beta;
+            if (length <= nxt_length) { min_length = length; sspace = space2; }
+        }
+    }
+    *sspace_out = (unsigned long long)sspace;
+    *delta_out = (size_t)min_length;
+}
 
 // A device buffer that only grows.
 struct DevBuf {
@@ -82,8 +155,18 @@ struct cbp_context {
     size_t query_len = 0;
     float score_thld = 0.f;
     float logE_thld = 0.f;
+    // Karlin-Altschul parameters (cother.par: [UNGAPPED], [GAPPED_A_1])
+    float ref_lambda = 1.116276f, ref_K = 0.115812f;
+    float gap_lambda = 0.561132f, gap_K = 0.001488f, gap_alpha = 0.5f, gap_beta = -1.0f;
+    DevBuf nnweights;
     // working buffers
     DevBuf scores, modscores, btck, bandbuf, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
+    DevBuf hitrecs;
+    // results of the last process() call, all slabs
+    std::vector<float> h_recs;
+    unsigned long long searchspace = 0;
+    size_t delta_length = 0;
+    float query_eno = 0.f;
     // last slab
     long long last_col0 = 0;
     int last_ncols = 0;
@@ -326,6 +409,9 @@ int cbp_create(int device, const cbp_options* opt, const float* ss_table, size_t
             for (auto& e : c->ev) CBP_CUDA(cudaEventCreate(&e));
             std::memcpy(c->sstab_h, ss_table, sizeof(c->sstab_h));
             build_dms_table(c->dmstab_h);
+            c->nnweights.reserve(sizeof(kNNWeightsTable));
+            CBP_CUDA(cudaMemcpy(c->nnweights.p, kNNWeightsTable, sizeof(kNNWeightsTable),
+                                cudaMemcpyHostToDevice));
             c->sstab.reserve(sizeof(c->sstab_h));
             c->dmstab.reserve(sizeof(c->dmstab_h));
             CBP_CUDA(cudaMemcpy(c->sstab.p, c->sstab_h, sizeof(c->sstab_h), cudaMemcpyHostToDevice));
@@ -349,7 +435,7 @@ int cbp_destroy(cbp_context* c)
     c->db.release();
     c->query.release();
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax, &c->dpcoords,
-                      &c->dprecs, &c->passidx, &c->passdst, &c->passcnt})
+                      &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights})
         b->release();
     c->sstab.release();
     c->dmstab.release();
@@ -408,6 +494,18 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         c->launches = 0;
         for (float& m : c->stage_ms) m = 0.f;
         for (uint64_t& m : c->stage_launches) m = 0;
+        c->h_recs.clear();
+        c->query_eno = *reinterpret_cast<const float*>(qbeg[fENO]);
+        {
+            // effective search space (AbstractScoreMatrix::ComputeLengthAdjustment);
+            // the query length and the database totals default to this
+            // query and this chunk when not set
+            const size_t m = c->query_len ? c->query_len : (size_t)Lq;
+            const unsigned long long n = c->db_len ? c->db_len : (unsigned long long)c->db.view.N;
+            const size_t N = c->n_seqs ? c->n_seqs : (size_t)c->db.view.P;
+            length_adjustment(c->gap_lambda, c->gap_K, c->gap_alpha, c->gap_beta, m, n, N,
+                              &c->searchspace, &c->delta_length);
+        }
 
         std::vector<Slab> slabs = plan_slabs(c, Lq);
         size_t maxcols = 0, maxprof = 0;
@@ -489,6 +587,45 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             c->last_Lq = Lq;
             c->last_nprof = d.nprof;
             c->last_npass = npass;
+
+            // statistics and E-values of the passed pairs of this slab
+            if (npass > 0) {
+                c->hitrecs.reserve((size_t)npass * kRecFloats * sizeof(float));
+                StatsArgs st;
+                st.scores = a.scores;
+                st.ld = a.ld;
+                st.Lq = Lq;
+                st.col0 = s.col0;
+                st.p0 = s.p0;
+                st.db = c->db.view;
+                st.qaa = c->query.view.aa;
+                st.qeno = c->query_eno;
+                st.x_uninf = c->opt.x_uninf;
+                st.pass_idx = c->passidx.as<int>();
+                st.pass_dst = c->passdst.as<long long>();
+                st.recs = c->dprecs.as<Dp1Rec>();
+                st.out = c->hitrecs.as<float>();
+                st.nnweights = c->nnweights.as<float>();
+                st.ssemodel = c->opt.ssemodel;
+                st.searchspace = (float)c->searchspace;
+                st.ref_lambda = c->ref_lambda;
+                st.ref_K = c->ref_K;
+                st.exp_gapped_lambda = c->gap_lambda;
+                st.exp_gapped_K = c->gap_K;
+                CBP_CUDA(cudaEventRecord(c->ev[4], c->stream));
+                launch_stats(st, npass, c->stream);
+                CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
+                c->launches += 1;
+                c->stage_launches[3] += 1;
+                const size_t off = c->h_recs.size();
+                c->h_recs.resize(off + (size_t)npass * kRecFloats);
+                CBP_CUDA(cudaMemcpyAsync(c->h_recs.data() + off, c->hitrecs.p,
+                                         (size_t)npass * kRecFloats * sizeof(float),
+                                         cudaMemcpyDeviceToHost, c->stream));
+                CBP_CUDA(cudaStreamSynchronize(c->stream));
+                CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+                c->stage_ms[3] += ms;
+            }
         }
         CBP_CUDA(cudaStreamSynchronize(c->stream));
     });
@@ -551,6 +688,44 @@ int cbp_read_btck(cbp_context* c, uint8_t* btck, size_t ld)
         if (ld < (size_t)c->last_ncols) throw Error(CBP_ERR_ARG, "ld smaller than the slab width");
         CBP_CUDA(cudaMemcpy2D(btck, ld, c->btck.p, c->last_ld, (size_t)c->last_ncols, c->last_Lq,
                               cudaMemcpyDeviceToHost));
+    });
+}
+
+int cbp_get_hit_records(cbp_context* c, float* recs, size_t max_records, size_t* nrecords)
+{
+    return guarded([&] {
+        check_ctx(c);
+        const size_t n = c->h_recs.size() / kRecFloats;
+        if (nrecords) *nrecords = n;
+        if (recs) {
+            if (max_records < n) throw Error(CBP_ERR_ARG, "record buffer too small");
+            std::memcpy(recs, c->h_recs.data(), c->h_recs.size() * sizeof(float));
+        }
+    });
+}
+
+int cbp_get_search_space(cbp_context* c, uint64_t* search_space, size_t* delta_length)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (search_space) *search_space = c->searchspace;
+        if (delta_length) *delta_length = c->delta_length;
+    });
+}
+
+int cbp_set_karlin_altschul(cbp_context* c, float ungapped_lambda, float ungapped_k,
+                            float gapped_lambda, float gapped_k, float gapped_alpha, float gapped_beta)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!(ungapped_lambda > 0.f && ungapped_k > 0.f && gapped_lambda > 0.f && gapped_k > 0.f))
+            throw Error(CBP_ERR_ARG, "lambda and K must be positive");
+        c->ref_lambda = ungapped_lambda;
+        c->ref_K = ungapped_k;
+        c->gap_lambda = gapped_lambda;
+        c->gap_K = gapped_k;
+        c->gap_alpha = gapped_alpha;
+        c->gap_beta = gapped_beta;
     });
 }
 

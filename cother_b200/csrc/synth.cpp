@@ -14,6 +14,10 @@
 // filled with penalty distances (DSTSEP6=12 or DSTGAPL=24; DSTFREE=3,
 // DSTNPOS=12, DSTSEGM=6 as in src/env/options.txt).
 //
+// Amino acids are stored as letters and SS states as ' ', 'e', 'h' (the
+// reference's text reader keeps residue letters and lower-case SS codes,
+// src/libmycu/cupro/IOProfileModelTxt.cu:438,1029; src/liblib/alpha.cpp:12-14).
+//
 // Two distance sources are generated:
 //  * "observed" (database profiles): a C-beta random walk with 3.8 A steps,
 //    pairwise Euclidean distances rounded to integers;
@@ -192,8 +196,11 @@ void GenProfile(int p, int P, long long N, const int* lens, const long long* sta
     }
 
     // per-position fields
+    // Dirichlet(0.5 per letter) centred on the profile background, so that
+    // the target frequencies average to the background (and unrelated
+    // profiles score below zero on average, as real profiles do)
     double at[kNAA];
-    for (int i = 0; i < kNAA; i++) at[i] = 0.5;
+    for (int i = 0; i < kNAA; i++) at[i] = 0.5 * kNAA * bk[i];
     for (int k = 0; k < L; k++) {
         const long long n = s0 + k;
         double tf[kNAA], sp[3];
@@ -204,7 +211,7 @@ void GenProfile(int p, int P, long long N, const int* lens, const long long* sta
             f.tf[(long long)i * N + n] = (float)v;
             if (tf[i] > tf[amax]) amax = i;
         }
-        f.aa[n] = (int8_t)amax;
+        f.aa[n] = (int8_t)"ARNDCQEGHILKMFPSTWYV"[amax];
         const double a3[3] = {1.0, 1.0, 1.0};
         rng.dirichlet(a3, 3, sp);
         int smax = 0;
@@ -212,7 +219,7 @@ void GenProfile(int p, int P, long long N, const int* lens, const long long* sta
             f.ss[(long long)i * N + n] = (float)sp[i];
             if (sp[i] > sp[smax]) smax = i;
         }
-        f.ssstate[n] = (int8_t)smax;
+        f.ssstate[n] = (int8_t)" eh"[smax];
         f.addrpro[n] = p;
     }
 

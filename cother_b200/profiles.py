@@ -62,9 +62,10 @@ NFIELDS = PMV_SSSTATE + 1              # 181
 
 DST_NODATA = 255.0
 
-# amino-acid alphabet of the reference (src/liblib/alpha.cpp: gAlphabet)
-AA_ALPHABET = "ARNDCQEGHILKMFPSTWYVBZJX*-"
-SS_ALPHABET = "CEH"
+# amino acids are stored as letters, SS states as ' ', 'e', 'h'
+# (src/liblib/alpha.cpp:12-14)
+AA_ALPHABET = "ARNDCQEGHILKMFPSTWYV"
+SS_CODES = " eh"
 
 
 @dataclass
@@ -172,4 +173,4 @@ class ProfileSet:
 
     def sequence(self, p: int) -> str:
         s0 = int(self.starts[p])
-        return "".join(AA_ALPHABET[int(c)] for c in self.aa[s0:s0 + int(self.lens[p])])
+        return bytes(self.aa[s0:s0 + int(self.lens[p])].astype(np.uint8)).decode()

@@ -155,6 +155,33 @@ void cbp_score_threshold(size_t query_len, uint64_t db_len, float evalue,
                          float gapped_lambda, float gapped_k,
                          float* score_threshold, float* log_evalue_threshold);
 
+/* Number of floats of one hit record: the fields of TDP2OutputAlnData
+ * (src/libmycu/cuss/CuBatchSS_com.h:45-71) in this order: score,
+ * original profile number*, offset in the phase-2 position space*,
+ * #positive scores, beginning coords*, end coords*, estimated gapped lambda,
+ * estimated gapped K, log E-value, log E-value of the pair, min score, max
+ * score, expected score, relative entropy, lambda, K, #identities, #gaps
+ * (* = uint32 stored in the float's bits; coordinates packed (x<<16)|y). */
+#define CBP_REC_FLOATS 18
+
+/* Hit records of the last cbp_process() call, one per pair that passed
+ * phase 1, over all slabs, in database order. With recs == NULL only the
+ * count is returned. (The reference hands the same array to its finalizer,
+ * src/libmycu/cupro/CuBatchProcessing.cu:599-697.) */
+int cbp_get_hit_records(cbp_context* ctx, float* recs, size_t max_records, size_t* nrecords);
+
+/* Effective search space and length adjustment of the last cbp_process()
+ * call (AbstractScoreMatrix::ComputeLengthAdjustment,
+ * src/libpro/srcsco/AbstractScoreMatrix.cpp:247-393). */
+int cbp_get_search_space(cbp_context* ctx, uint64_t* search_space, size_t* delta_length);
+
+/* Karlin-Altschul parameters of the statistical configuration (cother.par:
+ * [UNGAPPED] lambda, K; [GAPPED_A_1] lambda, K, alpha, beta). Defaults are
+ * the reference's shipped values. */
+int cbp_set_karlin_altschul(cbp_context* ctx, float ungapped_lambda, float ungapped_k,
+                            float gapped_lambda, float gapped_k, float gapped_alpha,
+                            float gapped_beta);
+
 /* Limit the number of database positions processed per slab (0 = plan by
  * the memory budget). Used to exercise multi-slab processing. */
 int cbp_set_max_slab_positions(cbp_context* ctx, size_t max_positions);

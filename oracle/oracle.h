@@ -69,15 +69,6 @@ void orc_score_matrix_mt(int nthreads, int Lq, const float* q_tf, const float* q
                          long long col0, long long ncols,
                          float* scores, float* modscores, long long ld);
 
-#ifdef __cplusplus
-}
-#endif
-
-#endif
-
-#ifdef __cplusplus
-extern "C" {
-#endif
 
 /* ------------------------------------------------------------------------
  * Phase-1 DP (src/libmycu/cudp/CuBatchDP_init_btck.cu:65-494) for one
@@ -106,6 +97,39 @@ int orc_dp1_finalize(int Lq, int Ld, const float* S, long long lds, const uint8_
 void orc_score_threshold(size_t nqyposs, size_t dbsize, float evalue, float gapped_lambda,
                          float gapped_k, float* scorethld, float* logevthld);
 
+/* ------------------------------------------------------------------------
+ * Statistics and significance (oracle_stats.c).
+ */
+float orc_expf(float x);
+float orc_lgammaf(float x);
+float orc_lbetaincf(float a, float b, float x);
+float orc_lgammainc_Qf(float a, float x);
+
+/* 641 counts of rint(32*clamp(score,-10,10)) + 320 over a pair's cells */
+void orc_score_histogram(int Lq, int Ld, const float* S, long long lds, const char* qaa,
+                         const char* daa, int xuninf, int* counts);
+
+/* out[6] = min, max, E, H, lambda, K; up[21] = unscaled probabilities */
+void orc_stat_params(const int* counts, float* out, float* up);
+
+typedef struct orc_sig_params {
+    int ssemodel;
+    float searchspace;
+    float ref_lambda, ref_K;                 /* [UNGAPPED] of cother.par */
+    float exp_gapped_lambda, exp_gapped_K;   /* [GAPPED_A_1] of cother.par */
+    const float* nnweights;                  /* 93 network weights */
+} orc_sig_params;
+
+void orc_length_adjustment(float lambda, float K, float alpha, float beta, size_t m,
+                           unsigned long long n, size_t N, unsigned long long* sspace_out,
+                           size_t* delta_out);
+
+/* out4 = lambda_est, K_est, log E, log E per pair */
+void orc_significance(const orc_sig_params* sp, int Lq, int Ld, float qeno, float deno,
+                      float score, float psts, float lambda, float K, float* out4);
+
 #ifdef __cplusplus
 }
+#endif
+
 #endif

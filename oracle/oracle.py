@@ -180,3 +180,85 @@ def score_threshold(qlen, dbsize, evalue=10.0, lam=0.561132, K=0.001488):
     lib().orc_score_threshold(int(qlen), int(dbsize), float(evalue), float(lam), float(K),
                               ctypes.byref(a), ctypes.byref(b))
     return a.value, b.value
+
+
+# ---------------------------------------------------------------------------
+# statistics
+_GOLDEN = os.path.join(os.path.dirname(HERE), "tests", "golden")
+
+
+class SigParams(ctypes.Structure):
+    _fields_ = [("ssemodel", ctypes.c_int), ("searchspace", ctypes.c_float),
+                ("ref_lambda", ctypes.c_float), ("ref_K", ctypes.c_float),
+                ("exp_gapped_lambda", ctypes.c_float), ("exp_gapped_K", ctypes.c_float),
+                ("nnweights", ctypes.c_void_p)]
+
+
+def _stats_lib():
+    L = lib()
+    if not getattr(L, "_stats_bound", False):
+        L.orc_expf.restype = ctypes.c_float
+        L.orc_expf.argtypes = [ctypes.c_float]
+        L.orc_lgammaf.restype = ctypes.c_float
+        L.orc_lgammaf.argtypes = [ctypes.c_float]
+        L.orc_lbetaincf.restype = ctypes.c_float
+        L.orc_lbetaincf.argtypes = [ctypes.c_float] * 3
+        L.orc_lgammainc_Qf.restype = ctypes.c_float
+        L.orc_lgammainc_Qf.argtypes = [ctypes.c_float] * 2
+        L.orc_score_histogram.restype = None
+        L.orc_score_histogram.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.orc_stat_params.restype = None
+        L.orc_stat_params.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_significance.restype = None
+        L.orc_significance.argtypes = [ctypes.POINTER(SigParams), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_float, ctypes.c_float, ctypes.c_void_p]
+        L.orc_length_adjustment.restype = None
+        L.orc_length_adjustment.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                            ctypes.c_float, ctypes.c_size_t, ctypes.c_ulonglong,
+                                            ctypes.c_size_t, ctypes.POINTER(ctypes.c_ulonglong),
+                                            ctypes.POINTER(ctypes.c_size_t)]
+        L._stats_bound = True
+    return L
+
+
+def cother_par():
+    import json
+    return json.load(open(os.path.join(_GOLDEN, "cother_par.json")))
+
+
+def nn_weights():
+    return np.load(os.path.join(_GOLDEN, "nn_weights.npy")).astype(np.float32)
+
+
+def length_adjustment(m, n, N):
+    par = cother_par()["GAPPED_A_1"]
+    ss, dl = ctypes.c_ulonglong(), ctypes.c_size_t()
+    _stats_lib().orc_length_adjustment(par["Lambda"], par["K"], par["Alpha"], par["Beta"], int(m),
+                                       int(n), int(N), ctypes.byref(ss), ctypes.byref(dl))
+    return ss.value, dl.value
+
+
+def pair_statistics(S, qaa, daa, score, psts, Lq, Ld, qeno, deno, searchspace, ssemodel=2,
+                    xuninf=1):
+    """(lambda_est, K_est, logE, logEpA, min, max, E, H, lambda, K) for one
+    passed pair; S is its [Lq][Ld] score sub-matrix."""
+    L = _stats_lib()
+    S = np.ascontiguousarray(S, np.float32)
+    qa = np.ascontiguousarray(qaa, np.int8)
+    da = np.ascontiguousarray(daa, np.int8)
+    counts = np.zeros(641, np.int32)
+    L.orc_score_histogram(Lq, Ld, S.ctypes.data, S.shape[1], qa.ctypes.data, da.ctypes.data,
+                          int(xuninf), counts.ctypes.data)
+    prm = np.zeros(6, np.float32)
+    up = np.zeros(21, np.float32)
+    L.orc_stat_params(counts.ctypes.data, prm.ctypes.data, up.ctypes.data)
+    par = cother_par()
+    w = nn_weights()
+    sp = SigParams(int(ssemodel), float(searchspace), par["UNGAPPED"]["Lambda"], par["UNGAPPED"]["K"],
+                   par["GAPPED_A_1"]["Lambda"], par["GAPPED_A_1"]["K"], w.ctypes.data)
+    o4 = np.zeros(4, np.float32)
+    L.orc_significance(ctypes.byref(sp), int(Lq), int(Ld), float(qeno), float(deno), float(score),
+                       float(psts), float(prm[4]), float(prm[5]), o4.ctypes.data)
+    return np.concatenate([o4, prm]), counts

@@ -7,6 +7,11 @@ tests and the benchmark need from it is committed:
 * ssss.npy       -- the SS score table of src/env/ssss (30x30, full
                     symmetric, float32 as parsed by the reference's
                     VirtScores::ReadScoresHelper, src/libpro/srcpro/VirtScores.cpp:44)
+* nn_weights.npy -- the 93 parameters of the significance networks and the
+                    SS18 adjustments (static table SSE_NN_WEIGHTS_ of
+                    src/libmycu/cupro/CuDeviceMemory.cu:43-80)
+* cother_par.json -- the [UNGAPPED] and [GAPPED_A_1] lambda, K, alpha, beta
+                    of src/env/cother.par
 * ddms_ref.npz   -- DDMS golden vectors: seeded list pairs and the value
                     returned by the reference's own CPU restatement
                     (cother-scores-optimizer/ddms.cxx:388-436, built by
@@ -37,6 +42,31 @@ def parse_ssss(path):
     return T
 
 
+def parse_nn_weights(path):
+    import re
+    text = open(path).read()
+    i = text.index("SSE_NN_WEIGHTS_[]")
+    j = text.index("};", i)
+    body = re.sub(r"//[^\n]*", "", text[i:j].split("{", 1)[1])
+    vals = [np.float32(v.rstrip("f")) for v in re.findall(r"[-+]?[0-9]*\.?[0-9]+(?:[eE][-+]?[0-9]+)?f?", body)]
+    w = np.array(vals, np.float32)
+    assert len(w) == 93, len(w)
+    return w
+
+
+def parse_cother_par(path):
+    out, sec = {}, None
+    for ln in open(path):
+        ln = ln.strip()
+        if ln.startswith("["):
+            sec = ln.strip("[]")
+            out[sec] = {}
+        elif "=" in ln and sec and not ln.startswith("#"):
+            k, v = [x.strip() for x in ln.split("=", 1)]
+            out[sec][k] = float(v)
+    return out
+
+
 def ddms_vectors(n_pairs=400, seed=99):
     from oracle import oracle as O
     from cother_b200 import synth
@@ -60,6 +90,12 @@ def ddms_vectors(n_pairs=400, seed=99):
 if __name__ == "__main__":
     T = parse_ssss(os.path.join(REF, "src/env/ssss"))
     np.save(os.path.join(HERE, "ssss.npy"), T)
+    np.save(os.path.join(HERE, "nn_weights.npy"),
+            parse_nn_weights(os.path.join(REF, "src/libmycu/cupro/CuDeviceMemory.cu")))
+    import json
+    par = parse_cother_par(os.path.join(REF, "src/env/cother.par"))
+    json.dump({k: par[k] for k in ("UNGAPPED", "GAPPED_A_1")},
+              open(os.path.join(HERE, "cother_par.json"), "w"), indent=1)
     qa, da, ref = ddms_vectors()
     np.savez_compressed(os.path.join(HERE, "ddms_ref.npz"), qlists=qa, dlists=da, ref=ref)
     print("ssss", T.shape, "ddms pairs", len(ref), "scored", int((ref != -777).sum()))
