@@ -82,6 +82,7 @@ def load_library(path: str | None = None):
                                        ctypes.POINTER(f32)]),
         "cbp_get_hit_records": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_get_search_space": (i32, [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(sz)]),
+        "cbp_get_alignments": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_set_karlin_altschul": (i32, [vp, f32, f32, f32, f32, f32, f32]),
         "cbp_stage_times": (i32, [vp, vp, i32]),
         "cbp_launch_count": (i32, [vp, ctypes.POINTER(ctypes.c_uint64)]),
@@ -241,6 +242,34 @@ class BatchProcessing:
         out = np.zeros((n.value, REC_FLOATS), np.float32)
         if n.value:
             _check(L.cbp_get_hit_records(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
+
+    def alignment_rows(self) -> np.ndarray:
+        """The 5 alignment rows of the last search (uint8 [5][length])."""
+        L = load_library()
+        n = ctypes.c_size_t()
+        _check(L.cbp_get_alignments(self._h, None, 0, ctypes.byref(n)))
+        rows = np.zeros((5, max(n.value, 1)), np.uint8)
+        if n.value:
+            _check(L.cbp_get_alignments(self._h, rows.ctypes.data, rows.shape[1], ctypes.byref(n)))
+        return rows[:, :n.value]
+
+    def alignments(self, query_len: int):
+        """Per hit: (query, middle, target, query SS, target SS) strings, or
+        None for hits that were not realigned."""
+        recs = records_table(self.hit_records())
+        rows = self.alignment_rows()
+        out = []
+        alnlen = recs["log_evalue_pair"].view(np.int32)
+        for k in range(len(recs["score"])):
+            n = int(alnlen[k])
+            if n <= 0:
+                out.append(None)
+                continue
+            p = int(recs["org_pro_no"][k])
+            Ld = int(self._db.lens[p])
+            term = int(recs["pro_new_dst"][k]) + k * query_len + Ld + query_len - 1
+            out.append(tuple(bytes(rows[r, term - n:term]).decode() for r in range(5)))
         return out
 
     def search_space(self):

@@ -31,8 +31,10 @@ CUDA_SOURCES = [
     "score_kernel.cu",
     "dp1_kernel.cu",
     "stats_kernel.cu",
+    "map_kernel.cu",
 ]
 CUDA_HEADERS = [
+    "map_kernel.cuh",
     "stats_kernel.cuh",
     "common.cuh",
     "cbmath.cuh",

@@ -18,6 +18,7 @@
 #include "score_kernel.cuh"
 #include "dp1_kernel.cuh"
 #include "stats_kernel.cuh"
+#include "map_kernel.cuh"
 
 namespace cbp {
 
@@ -161,7 +162,11 @@ struct cbp_context {
     DevBuf nnweights;
     // working buffers
     DevBuf scores, modscores, btck, bandbuf, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
-    DevBuf hitrecs;
+    DevBuf hitrecs, fb2, strip2, btck2, alnbuf;
+    std::vector<char> h_alns[5];
+    long long base_len = 0, base_npass = 0;   // running phase-2 offsets over slabs
+    long long last_ld2 = 0, last_npos2 = 0;
+    bool score_thld_set = false, logE_thld_set = false;
     // results of the last process() call, all slabs
     std::vector<float> h_recs;
     unsigned long long searchspace = 0;
@@ -340,7 +345,10 @@ std::vector<Slab> plan_slabs(const cbp_context* c, int Lq)
     const int P = (int)db.h_plen.size();
     // bytes per slab position: scores + modscores + backtrack byte per query
     // position, the DP band strip and per-profile records
-    const size_t per_pos = (size_t)Lq * 9 + 5 * 4 + 64;
+    // scores 4 + modscores 4 + phase-1 backtrack 1, and the phase-2 buffers
+    // for the worst case of every profile realigned: forward-backward 4 +
+    // MAP backtrack 1 + alignment rows 5; strips and records per position
+    const size_t per_pos = (size_t)Lq * 19 + 10 * 4 + 128;
     size_t cap = c->mem_budget / per_pos;
     if (c->max_slab_positions) cap = std::min(cap, c->max_slab_positions);
     cap = std::min<size_t>(cap, (size_t)1 << 30);
@@ -435,7 +443,8 @@ int cbp_destroy(cbp_context* c)
     c->db.release();
     c->query.release();
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax, &c->dpcoords,
-                      &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights})
+                      &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
+                      &c->fb2, &c->strip2, &c->btck2, &c->alnbuf})
         b->release();
     c->sstab.release();
     c->dmstab.release();
@@ -458,12 +467,12 @@ int cbp_set_query_len(cbp_context* c, size_t qlen)
 
 int cbp_set_score_threshold(cbp_context* c, float t)
 {
-    return guarded([&] { check_ctx(c); c->score_thld = t; });
+    return guarded([&] { check_ctx(c); c->score_thld = t; c->score_thld_set = true; });
 }
 
 int cbp_set_logE_threshold(cbp_context* c, float t)
 {
-    return guarded([&] { check_ctx(c); c->logE_thld = t; });
+    return guarded([&] { check_ctx(c); c->logE_thld = t; c->logE_thld_set = true; });
 }
 
 int cbp_set_max_slab_positions(cbp_context* c, size_t n)
@@ -495,6 +504,10 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         for (float& m : c->stage_ms) m = 0.f;
         for (uint64_t& m : c->stage_launches) m = 0;
         c->h_recs.clear();
+        for (auto& r : c->h_alns) r.clear();
+        c->base_len = 0;
+        c->base_npass = 0;
+        c->last_ld2 = c->last_npos2 = 0;
         c->query_eno = *reinterpret_cast<const float*>(qbeg[fENO]);
         {
             // effective search space (AbstractScoreMatrix::ComputeLengthAdjustment);
@@ -505,6 +518,12 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             const size_t N = c->n_seqs ? c->n_seqs : (size_t)c->db.view.P;
             length_adjustment(c->gap_lambda, c->gap_K, c->gap_alpha, c->gap_beta, m, n, N,
                               &c->searchspace, &c->delta_length);
+            // thresholds not set by the caller follow from EVAL as the
+            // reference's job dispatcher derives them
+            float sthld = 0.f, lthld = 0.f;
+            cbp_score_threshold(m, n, c->opt.eval, c->gap_lambda, c->gap_K, &sthld, &lthld);
+            if (!c->score_thld_set) c->score_thld = sthld;
+            if (!c->logE_thld_set) c->logE_thld = lthld;
         }
 
         std::vector<Slab> slabs = plan_slabs(c, Lq);
@@ -617,14 +636,87 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
                 c->launches += 1;
                 c->stage_launches[3] += 1;
+
+                // phase-2 MAP realignment of the pairs within the E-value
+                // threshold (in the phase-2 column space of this slab)
+                long long npos2 = 0;
+                CBP_CUDA(cudaMemcpyAsync(&npos2, c->passcnt.as<char>() + 8, sizeof(long long),
+                                         cudaMemcpyDeviceToHost, c->stream));
+                CBP_CUDA(cudaStreamSynchronize(c->stream));
+                const long long ld2 = align_up(npos2, 32);
+                const long long alnstride = align_up(npos2 + (long long)npass * Lq, 32);
+                if (c->opt.mapaln) {
+                    c->fb2.reserve((size_t)Lq * ld2 * sizeof(float));
+                    c->strip2.reserve(5 * (size_t)ld2 * sizeof(float));
+                    c->btck2.reserve((size_t)Lq * ld2);
+                    c->alnbuf.reserve(5 * (size_t)alnstride);
+                    MapArgs mp;
+                    mp.scores = a.scores;
+                    mp.modscores = a.modscores;
+                    mp.ld = a.ld;
+                    mp.Lq = Lq;
+                    mp.col0 = s.col0;
+                    mp.p0 = s.p0;
+                    mp.db = c->db.view;
+                    mp.qtrn = c->query.view.trn;
+                    mp.qaa = c->query.view.aa;
+                    mp.qsss = c->query.view.sss;
+                    mp.printsss = c->opt.ssswgt > 0.0f;
+                    mp.modscores_inuse = (c->opt.ssswgt > 0.0f || c->opt.cvswgt > 0.0f) ? 1 : 0;
+                    mp.minpp = c->opt.minpp;
+                    mp.logevthld = c->logE_thld;
+                    mp.npass = npass;
+                    mp.pass_idx = c->passidx.as<int>();
+                    mp.pass_dst = c->passdst.as<long long>();
+                    mp.recs = c->hitrecs.as<float>();
+                    mp.fb = c->fb2.as<float>();
+                    mp.strip = c->strip2.as<float>();
+                    mp.btck = c->btck2.as<uint8_t>();
+                    mp.ld2 = ld2;
+                    mp.alns = c->alnbuf.as<char>();
+                    mp.alnstride = alnstride;
+                    CBP_CUDA(cudaMemsetAsync(c->alnbuf.p, 0, 5 * (size_t)alnstride, c->stream));
+                    CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
+                    launch_map(mp, c->stream);
+                    CBP_CUDA(cudaEventRecord(c->ev[7], c->stream));
+                    c->launches += 1;
+                    c->stage_launches[4] += 1;
+                    c->last_ld2 = ld2;
+                    c->last_npos2 = npos2;
+                }
                 const size_t off = c->h_recs.size();
                 c->h_recs.resize(off + (size_t)npass * kRecFloats);
                 CBP_CUDA(cudaMemcpyAsync(c->h_recs.data() + off, c->hitrecs.p,
                                          (size_t)npass * kRecFloats * sizeof(float),
                                          cudaMemcpyDeviceToHost, c->stream));
+                // this slab's alignment rows go to the running offset of
+                // the whole result (slot of pair K at newDst + K*Lq)
+                const long long shift = c->base_len + c->base_npass * (long long)Lq;
+                const long long slablen = npos2 + (long long)npass * Lq;
+                for (int row = 0; row < 5; row++) {
+                    c->h_alns[row].resize((size_t)(shift + slablen), 0);
+                    if (c->opt.mapaln)
+                        CBP_CUDA(cudaMemcpyAsync(c->h_alns[row].data() + shift,
+                                                 c->alnbuf.as<char>() + (size_t)row * alnstride,
+                                                 (size_t)slablen, cudaMemcpyDeviceToHost, c->stream));
+                }
                 CBP_CUDA(cudaStreamSynchronize(c->stream));
                 CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
                 c->stage_ms[3] += ms;
+                if (c->opt.mapaln) {
+                    CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]));
+                    c->stage_ms[4] += ms;
+                }
+                // phase-2 offsets of this slab's pairs become offsets in the
+                // whole result
+                for (size_t i = off; i < c->h_recs.size(); i += kRecFloats) {
+                    uint32_t v;
+                    std::memcpy(&v, &c->h_recs[i + rProNewDst], 4);
+                    v += (uint32_t)c->base_len;
+                    std::memcpy(&c->h_recs[i + rProNewDst], &v, 4);
+                }
+                c->base_len += npos2;
+                c->base_npass += npass;
             }
         }
         CBP_CUDA(cudaStreamSynchronize(c->stream));
@@ -700,6 +792,19 @@ int cbp_get_hit_records(cbp_context* c, float* recs, size_t max_records, size_t*
         if (recs) {
             if (max_records < n) throw Error(CBP_ERR_ARG, "record buffer too small");
             std::memcpy(recs, c->h_recs.data(), c->h_recs.size() * sizeof(float));
+        }
+    });
+}
+
+int cbp_get_alignments(cbp_context* c, char* rows, size_t row_stride, size_t* length)
+{
+    return guarded([&] {
+        check_ctx(c);
+        const size_t n = c->h_alns[0].size();
+        if (length) *length = n;
+        if (rows) {
+            if (row_stride < n) throw Error(CBP_ERR_ARG, "row stride smaller than the alignment rows");
+            for (int r = 0; r < 5; r++) std::memcpy(rows + (size_t)r * row_stride, c->h_alns[r].data(), n);
         }
     });
 }

@@ -170,6 +170,18 @@ void cbp_score_threshold(size_t query_len, uint64_t db_len, float evalue,
  * src/libmycu/cupro/CuBatchProcessing.cu:599-697.) */
 int cbp_get_hit_records(cbp_context* ctx, float* recs, size_t max_records, size_t* nrecords);
 
+/* Alignment strings of the last cbp_process() call: 5 rows (query, middle,
+ * target, query SS, target SS) of *length bytes each, copied to
+ * rows[r * row_stride]. Hit k (record order) owns bytes
+ * [newDst_k + k*Lq, newDst_k + k*Lq + Ld_k + Lq) of every row, with its
+ * alignment right-aligned and 0-terminated at the slot's last byte; the
+ * alignment length is the int stored in the record's log-E-value-of-pair
+ * field after realignment (0 when the pair was not realigned). This is the
+ * layout the reference's finalizer reads
+ * (src/libmycu/cumapdp/CuBatchMAPDP_map_final.cu:190-330). With rows ==
+ * NULL only *length is returned. */
+int cbp_get_alignments(cbp_context* ctx, char* rows, size_t row_stride, size_t* length);
+
 /* Effective search space and length adjustment of the last cbp_process()
  * call (AbstractScoreMatrix::ComputeLengthAdjustment,
  * src/libpro/srcsco/AbstractScoreMatrix.cpp:247-393). */

@@ -262,3 +262,61 @@ def pair_statistics(S, qaa, daa, score, psts, Lq, Ld, qeno, deno, searchspace, s
     L.orc_significance(ctypes.byref(sp), int(Lq), int(Ld), float(qeno), float(deno), float(score),
                        float(psts), float(prm[4]), float(prm[5]), o4.ctypes.data)
     return np.concatenate([o4, prm]), counts
+
+
+# ---------------------------------------------------------------------------
+# phase-2 MAP realignment
+class MapIn(ctypes.Structure):
+    _fields_ = [("Lq", ctypes.c_int), ("Ld", ctypes.c_int), ("S", ctypes.c_void_p),
+                ("M", ctypes.c_void_p), ("lds", ctypes.c_longlong), ("qtrn", ctypes.c_void_p),
+                ("qts", ctypes.c_longlong), ("dtrn", ctypes.c_void_p), ("dts", ctypes.c_longlong),
+                ("epa", ctypes.c_float), ("minpp", ctypes.c_float), ("modscores", ctypes.c_int),
+                ("qaa", ctypes.c_void_p), ("daa", ctypes.c_void_p), ("qss", ctypes.c_void_p),
+                ("dss", ctypes.c_void_p), ("printsss", ctypes.c_int), ("qsssinuse", ctypes.c_int),
+                ("dsssinuse", ctypes.c_int)]
+
+
+class MapOut(ctypes.Structure):
+    _fields_ = [("fb", ctypes.c_void_p), ("btck", ctypes.c_void_p), ("aln", ctypes.c_void_p * 5),
+                ("maxlogprob", ctypes.c_float), ("logz", ctypes.c_float), ("mapmax", ctypes.c_float),
+                ("alnlen", ctypes.c_int), ("idts", ctypes.c_int), ("psts", ctypes.c_int),
+                ("gaps", ctypes.c_int), ("beg", ctypes.c_uint32), ("end", ctypes.c_uint32)]
+
+
+def map_pair(query, db, p, S, M, epa, minpp=0.28, modscores=True, printsss=True):
+    """MAP realignment of query vs profile p; S, M: the pair's [Lq][Ld]
+    scores and modular scores. Returns a dict (fb, btck, alignment rows,
+    counts, coordinates, logz, maxlogprob, mapmax)."""
+    L = lib()
+    if not getattr(L, "_map_bound", False):
+        L.orc_map_pair.restype = ctypes.c_int
+        L.orc_map_pair.argtypes = [ctypes.POINTER(MapIn), ctypes.POINTER(MapOut)]
+        L._map_bound = True
+    p = int(p)
+    Lq = query.npositions
+    Ld = int(db.lens[p])
+    s0 = int(db.starts[p])
+    S = np.ascontiguousarray(S, np.float32)
+    M = np.ascontiguousarray(M, np.float32)
+    qtrn = np.ascontiguousarray(query.trn, np.float32)
+    dtrn = np.ascontiguousarray(db.trn, np.float32)
+    qaa = np.ascontiguousarray(query.aa, np.int8)
+    daa = np.ascontiguousarray(db.aa[s0:s0 + Ld], np.int8)
+    qss = np.ascontiguousarray(query.ssstate, np.int8)
+    dss = np.ascontiguousarray(db.ssstate[s0:s0 + Ld], np.int8)
+    fb = np.zeros((Lq, Ld), np.float32)
+    bt = np.zeros((Lq, Ld), np.uint8)
+    bufs = [ctypes.create_string_buffer(Lq + Ld + 2) for _ in range(5)]
+    mi = MapIn(Lq, Ld, S.ctypes.data, M.ctypes.data, S.shape[1], qtrn.ctypes.data, qtrn.shape[1],
+               dtrn.ctypes.data + 4 * (s0 + p), dtrn.shape[1], float(epa), float(minpp),
+               int(modscores), qaa.ctypes.data, daa.ctypes.data, qss.ctypes.data, dss.ctypes.data,
+               int(printsss), 1, 1)
+    mo = MapOut()
+    mo.fb = fb.ctypes.data
+    mo.btck = bt.ctypes.data
+    for i in range(5):
+        mo.aln[i] = ctypes.cast(bufs[i], ctypes.c_void_p)
+    L.orc_map_pair(ctypes.byref(mi), ctypes.byref(mo))
+    return {"fb": fb, "btck": bt, "aln": [b.value.decode() for b in bufs], "alnlen": mo.alnlen,
+            "idts": mo.idts, "psts": mo.psts, "gaps": mo.gaps, "beg": mo.beg, "end": mo.end,
+            "logz": mo.logz, "maxlogprob": mo.maxlogprob, "mapmax": mo.mapmax}

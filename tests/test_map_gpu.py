@@ -1,0 +1,93 @@
+"""Phase-2 MAP realignment on the GPU vs the CPU oracle: identical
+alignment strings, identities, positives, gaps and coordinates."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _search(q, db, ss, thld=None, logethld=None, max_slab=0, **opt):
+    import cother_b200 as cb
+    o = cb.Options.defaults()
+    for k, v in opt.items():
+        setattr(o, k, v)
+    bp = cb.BatchProcessing(ss, o)
+    if thld is not None:
+        bp.set_score_threshold(thld)
+    if logethld is not None:
+        bp.set_logE_threshold(logethld)
+    if max_slab:
+        bp.set_max_slab_positions(max_slab)
+    bp.transfer_cpm_data(db)
+    bp.process_score_matrix(q)
+    return bp
+
+
+def _check_map(bp, oracle_lib, q, db, minpp=0.28, logethld=2.302585):
+    import cother_b200 as cb
+    recs = cb.records_table(bp.hit_records())
+    alns = bp.alignments(q.npositions)
+    sc, ms, first = bp.read_score_matrix(q.npositions, db.npositions)
+    assert first == 0
+    sspace, _ = bp.search_space()
+    nrealigned = 0
+    for k in range(len(recs["score"])):
+        p = int(recs["org_pro_no"][k])
+        s0, Ld = int(db.starts[p]), int(db.lens[p])
+        st, _ = oracle_lib.pair_statistics(sc[:, s0:s0 + Ld], q.aa, db.aa[s0:s0 + Ld],
+                                           recs["score"][k], 0.0, q.npositions, Ld, q.eno[0],
+                                           db.eno[p], sspace)
+        logE, epa = st[2], st[3]
+        assert np.float32(logE) == recs["log_evalue"][k]
+        if logethld < logE:
+            assert alns[k] is None
+            continue
+        m = oracle_lib.map_pair(q, db, p, sc[:, s0:s0 + Ld], ms[:, s0:s0 + Ld], epa, minpp=minpp)
+        if m["alnlen"] == 0:
+            assert alns[k] is None
+            continue
+        nrealigned += 1
+        assert alns[k] == tuple(m["aln"]), (p, alns[k][0][:40], m["aln"][0][:40])
+        assert recs["identities"][k] == m["idts"]
+        assert recs["psts"][k] == m["psts"]
+        assert recs["gaps"][k] == m["gaps"]
+        assert recs["beg_coords"][k] == m["beg"]
+        assert recs["end_coords"][k] == m["end"]
+    return nrealigned
+
+
+def test_map_homologs(oracle_lib, ss_table):
+    from cother_b200 import synth
+    q, db = synth.make_workload("q200_db1k", seed=5, ndb=48, homologs=0.25)
+    bp = _search(q, db, ss_table)
+    n = _check_map(bp, oracle_lib, q, db)
+    assert n >= 8
+    bp.close()
+
+
+def test_map_weak_pairs_and_minpp(oracle_lib, ss_table):
+    """A permissive threshold realigns random pairs too (short, gappy MAP
+    alignments, corner cells, logZ near zero); MINPP changes the DP."""
+    from cother_b200 import synth
+    q = synth.make_profiles([70], 91, True)
+    db = synth.make_profiles([40, 90, 33, 150, 64], 92, False)
+    for minpp in (0.28, 0.05):
+        bp = _search(q, db, ss_table, thld=-1.0, logethld=1e9, minpp=minpp)
+        _check_map(bp, oracle_lib, q, db, minpp=minpp, logethld=1e9)
+        bp.close()
+
+
+def test_map_multislab_offsets(oracle_lib, ss_table):
+    """Records and alignment rows of several slabs join into one result:
+    phase-2 offsets continue across slabs."""
+    import cother_b200 as cb
+    from cother_b200 import synth
+    q, db = synth.make_workload("q200_db1k", seed=8, ndb=36, homologs=0.3)
+    one = _search(q, db, ss_table)
+    many = _search(q, db, ss_table, max_slab=900)
+    r1, r2 = cb.records_table(one.hit_records()), cb.records_table(many.hit_records())
+    for f in ("score", "org_pro_no", "pro_new_dst", "log_evalue", "identities", "gaps"):
+        assert np.array_equal(r1[f], r2[f]), f
+    assert one.alignments(q.npositions) == many.alignments(q.npositions)
+    one.close()
+    many.close()
