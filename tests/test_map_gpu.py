@@ -30,12 +30,13 @@ def _check_map(bp, oracle_lib, q, db, minpp=0.28, logethld=2.302585):
     sc, ms, first = bp.read_score_matrix(q.npositions, db.npositions)
     assert first == 0
     sspace, _ = bp.search_space()
+    ph1, _ = bp.read_phase1()
     nrealigned = 0
     for k in range(len(recs["score"])):
         p = int(recs["org_pro_no"][k])
         s0, Ld = int(db.starts[p]), int(db.lens[p])
         st, _ = oracle_lib.pair_statistics(sc[:, s0:s0 + Ld], q.aa, db.aa[s0:s0 + Ld],
-                                           recs["score"][k], 0.0, q.npositions, Ld, q.eno[0],
+                                           recs["score"][k], ph1["psts"][p], q.npositions, Ld, q.eno[0],
                                            db.eno[p], sspace)
         logE, epa = st[2], st[3]
         assert np.float32(logE) == recs["log_evalue"][k]

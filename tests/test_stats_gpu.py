@@ -14,6 +14,7 @@ def _run(q, db, ss, thld, ssemodel=2, db_len=None, nseqs=None):
     import cother_b200 as cb
     o = cb.Options.defaults()
     o.ssemodel = ssemodel
+    o.mapaln = 0   # keep the records as the statistics stage leaves them
     bp = cb.BatchProcessing(ss, o)
     bp.set_score_threshold(thld)
     if db_len:
