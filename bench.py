@@ -32,7 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 DEFAULT_WORKLOAD = "q400_db50k"
-STAGES = ["score_matrix", "phase1_dp", "phase1_finalize"]
+STAGES = ["score_matrix", "phase1_dp", "phase1_finalize", "statistics", "map_realignment"]
 OPS_PER_DDMS_STEP = 50  # algorithmic ops of one 4-cell DDMS step (2 pair scores,
                         # 2 interpolations, 4 segment updates, 1 top-3 register)
 
@@ -135,25 +135,46 @@ def measured_peaks():
         return None
 
 
-def cpu_baseline(q, db, ss, seconds: float):
-    """Oracle (a port of the reference kernels) on the host cores, on a
-    bounded sample: the query against the first database profiles."""
+def oracle_pipeline(q, db, ss, nprof, nthreads, db_len, nseqs):
+    """The oracle's whole search path (score matrix, phase 1, statistics,
+    MAP realignment) for the query against the first `nprof` profiles."""
     from oracle import oracle as O
+    import cother_b200 as cb
+    ncols = int(db.starts[nprof - 1] + db.lens[nprof - 1]) if nprof < db.nprofiles else db.npositions
+    sc, ms = O.score_matrix(q, db, ss, ncols=ncols, nthreads=nthreads)
+    thld, lthld = cb.score_threshold(q.npositions, db_len)
+    sspace, _ = O.length_adjustment(q.npositions, db_len, nseqs)
+    rec, _ = O.dp1(q, db, sc, 0, 0, nprof, thld)
+    for p in np.nonzero(rec["passed"])[0]:
+        s0, Ld = int(db.starts[p]), int(db.lens[p])
+        st, _ = O.pair_statistics(sc[:, s0:s0 + Ld], q.aa, db.aa[s0:s0 + Ld], rec["score"][p],
+                                  rec["psts"][p], q.npositions, Ld, q.eno[0], db.eno[p], sspace)
+        if st[2] <= lthld:
+            O.map_pair(q, db, p, sc[:, s0:s0 + Ld], ms[:, s0:s0 + Ld], st[3])
+    return ncols
+
+
+def cpu_baseline(q, db, ss, seconds: float, db_len: int, nseqs: int):
+    """Oracle (a port of the reference kernels) on the host cores, on a
+    bounded sample: the query against the first database profiles, through
+    the whole path."""
     ncpu = os.cpu_count() or 1
-    # calibrate on a small sample, then size the timed sample
-    probe = int(min(db.npositions, 64))
+    # calibrate on a few profiles, then size the timed sample
+    probe = min(db.nprofiles, 4)
     t = time.perf_counter()
-    O.score_matrix(q, db, ss, ncols=probe, nthreads=ncpu)
+    cols = oracle_pipeline(q, db, ss, probe, ncpu, db_len, nseqs)
     dt = max(time.perf_counter() - t, 1e-3)
-    rate = q.npositions * probe / dt
-    ncols = int(min(db.npositions, max(probe, rate * seconds / q.npositions)))
+    rate = cols / dt
+    mean_len = float(db.lens.mean())
+    nprof = int(min(db.nprofiles, max(probe, rate * seconds / mean_len)))
     t = time.perf_counter()
-    O.score_matrix(q, db, ss, ncols=ncols, nthreads=ncpu)
+    cols = oracle_pipeline(q, db, ss, nprof, ncpu, db_len, nseqs)
     dt = time.perf_counter() - t
-    cells = q.npositions * ncols
+    cells = q.npositions * cols
     return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": ncpu, "kind": "port",
-            "sample": f"query {q.npositions} x first {ncols} database positions "
-                      f"({cells} cells, {dt:.1f} s), score-matrix stage"}
+            "sample": f"query {q.npositions} x first {nprof} database profiles ({cols} positions, "
+                      f"{cells} cells, {dt:.1f} s), whole path (score matrix, phase 1, "
+                      f"statistics, MAP), score matrix on {ncpu} threads"}
 
 
 def run_reference(args):
@@ -167,8 +188,10 @@ def run_reference(args):
     ndb = args.ndb or 200
     q, db = synth.make_workload(args.workload, seed=args.seed, ndb=ndb)
     vals = []
+    full = synth.db_lengths(args.workload, args.seed)
+    db_len, nseqs = int(full.sum()), len(full)
     for _ in range(max(1, args.warmup) + args.steps):
-        vals.append(cpu_baseline(q, db, ss, args.cpu_seconds / 3))
+        vals.append(cpu_baseline(q, db, ss, args.cpu_seconds / 3, db_len, nseqs))
     timed = vals[-args.steps:] if args.steps > 0 else vals
     v = float(np.mean([x["value"] for x in timed]))
     cb = dict(timed[-1])
@@ -176,7 +199,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "stages": ["score_matrix"]},
+            "config": {"workload": args.workload, "stages": STAGES},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -207,7 +230,8 @@ def main():
 
     bp = cb.BatchProcessing(ss, device=local)
     bp.transfer_cpm_data(db)
-    bp.set_db_details(Ndb * world, db.nprofiles * world)
+    db_len, nseqs = Ndb * world, db.nprofiles * world
+    bp.set_db_details(db_len, nseqs)
     bp.set_query_len(Lq)
 
     def barrier():
@@ -226,8 +250,14 @@ def main():
     kern_ms, launches = 0.0, 0
     score_ms, score_launches = 0.0, 0
     e0.record(stream)
+    d2h = 0
+    nhits = 0
     for _ in range(args.steps):
         bp.process_score_matrix(q)
+        recs = bp.hit_records()
+        rows = bp.alignment_rows()
+        d2h = recs.nbytes + rows.nbytes
+        nhits = len(recs)
         st = bp.stage_times()
         kern_ms += sum(st)
         score_ms += st[0]
@@ -270,10 +300,11 @@ def main():
                            "parallelism": f"dp{world} (database shard per GPU)"},
                 "e2e": {"value": e2e, "unit": "GCUPS",
                         "h2d_bytes_per_step": int(Lq * (4 * 20 + 4 * 3 + 4 * 100 + 2) + 4 * 7 * (Lq + 1)),
-                        "d2h_bytes_per_step": 0},
+                        "d2h_bytes_per_step": int(d2h)},
+                "hits": nhits,
                 "gpu_launches": launches, "roofline": roof, "clocks": clocks}
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds)
+            line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds, db_len, nseqs)
         print(json.dumps(line))
     bp.close()
     if dist is not None:
