@@ -140,7 +140,8 @@ def oracle_pipeline(q, db, ss, nprof, nthreads, db_len, nseqs):
     MAP realignment) for the query against the first `nprof` profiles."""
     from oracle import oracle as O
     import cother_b200 as cb
-    ncols = int(db.starts[nprof - 1] + db.lens[nprof - 1]) if nprof < db.nprofiles else db.npositions
+    db = db.subset(0, nprof)
+    ncols = db.npositions
     sc, ms = O.score_matrix(q, db, ss, ncols=ncols, nthreads=nthreads)
     thld, lthld = cb.score_threshold(q.npositions, db_len)
     sspace, _ = O.length_adjustment(q.npositions, db_len, nseqs)
