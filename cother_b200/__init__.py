@@ -83,6 +83,8 @@ def load_library(path: str | None = None):
         "cbp_get_hit_records": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_get_search_space": (i32, [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(sz)]),
         "cbp_get_alignments": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
+        "cbp_dp1_noalloc": (i32, [vp, sz, i32, vp, ctypes.c_longlong, i32, vp, vp, vp, i32, i32,
+                                  ctypes.c_longlong, vp, vp, vp, vp]),
         "cbp_set_karlin_altschul": (i32, [vp, f32, f32, f32, f32, f32, f32]),
         "cbp_stage_times": (i32, [vp, vp, i32]),
         "cbp_launch_count": (i32, [vp, ctypes.POINTER(ctypes.c_uint64)]),

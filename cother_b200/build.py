@@ -32,6 +32,7 @@ CUDA_SOURCES = [
     "dp1_kernel.cu",
     "stats_kernel.cu",
     "map_kernel.cu",
+    "dp1_noalloc.cu",
 ]
 CUDA_HEADERS = [
     "map_kernel.cuh",

@@ -30,6 +30,8 @@ enum {
 
 static thread_local std::string g_last_error;
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 // Parameters of the significance networks and of the SS18 model
 // adjustments (the reference's static table SSE_NN_WEIGHTS_,
 // src/libmycu/cupro/CuDeviceMemory.cu:43-80): E-network mu (4x5 + 5),

@@ -194,6 +194,47 @@ int cbp_set_karlin_altschul(cbp_context* ctx, float ungapped_lambda, float ungap
                             float gapped_lambda, float gapped_k, float gapped_alpha,
                             float gapped_beta);
 
+/* ------------------------------------------------------------------------
+ * Allocation-free phase-1 DP. This entry point has no counterpart in the
+ * reference.
+ *
+ * For callers that cannot allocate device memory when they run the search
+ * (their device memory belongs to their own pool allocator, or a cudaMalloc
+ * would synchronise the device where they enqueue work). The caller owns
+ * every input and output as device memory; the only scratch of the DP --
+ * the strip that carries each band's bottom row to the next band -- is a
+ * fixed array inside the library of 5 * CBP_NOALLOC_MAX_COLUMNS floats
+ * (1.25 MiB), which every GPU that loads the library keeps until the process
+ * exits. The call allocates and frees nothing.
+ *
+ * Inputs (device pointers, the layout of the other entry points):
+ *   scores     [query_len][ld] slab score matrix (column c = chunk position
+ *              first_column + c); ld <= CBP_NOALLOC_MAX_COLUMNS, else
+ *              CBP_ERR_LIMIT;
+ *   query_trn  [7][query_len+1] query transitions (entry r = into position r);
+ *   db_trn     [7][db_npos+db_nprof] chunk transitions, the beginning
+ *              vector of profile p at entry prof_start[p]+p;
+ *   prof_len, prof_start  [db_nprof] lengths and first positions;
+ *   profiles first_profile .. first_profile+nprof-1 are processed.
+ * Outputs (device): btck [query_len][ld] backtrack codes, max_scores and
+ * max_coords [nprof] (maximum MM score and its cell (x<<16)|y).
+ * The work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and the call returns after the launch.
+ *
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. All calls share the one scratch array and it
+ * keeps the last call's contents (the DP needs no zeroed scratch: the first
+ * band never reads the strip); calls whose work overlaps on the GPU race on
+ * it and must be serialised by the caller, e.g. on one stream. */
+#define CBP_NOALLOC_MAX_COLUMNS 65536
+int cbp_dp1_noalloc(const float* scores, size_t ld, int query_len, const float* query_trn,
+                    long long db_npos, int db_nprof, const float* db_trn,
+                    const int* prof_len, const long long* prof_start,
+                    int first_profile, int nprof, long long first_column,
+                    uint8_t* btck, float* max_scores, uint32_t* max_coords,
+                    void* stream);
+
 /* Limit the number of database positions processed per slab (0 = plan by
  * the memory budget). Used to exercise multi-slab processing. */
 int cbp_set_max_slab_positions(cbp_context* ctx, size_t max_positions);
