@@ -403,10 +403,15 @@ int cbp_create(int device, const cbp_options* opt, const float* ss_table, size_t
         if (!opt || !ss_table) throw Error(CBP_ERR_ARG, "null options or SS table");
         if (opt->cvswgt != 0.0f)
             throw Error(CBP_ERR_ARG, "CVSWGT > 0 (context-vector term) is not supported");
-        if (!(opt->ssswgt > 0.0f) || opt->ssswgt >= 1.0f)
-            throw Error(CBP_ERR_ARG, "SSSWGT must be in (0,1)");
-        if (opt->ddmswgt < 0.0f || opt->ddmswgt >= 1.0f) throw Error(CBP_ERR_ARG, "DDMSWGT must be in [0,1)");
+        // value ranges of src/libpro/srcpro/MOptions.cpp:76-141
+        if (!(opt->ssswgt >= 0.0f && opt->ssswgt < 1.0f))
+            throw Error(CBP_ERR_ARG, "SSSWGT must be in [0,1)");
+        if (!(opt->ddmswgt >= 0.0f && opt->ddmswgt < 1.0f))
+            throw Error(CBP_ERR_ARG, "DDMSWGT must be in [0,1)");
         if (opt->dstsegm < 1 || opt->dstsegm > 20) throw Error(CBP_ERR_ARG, "DSTSEGM must be in [1,20]");
+        if (opt->ssemodel < 0 || opt->ssemodel > 2) throw Error(CBP_ERR_ARG, "SSEMODEL must be 0, 1 or 2");
+        if (!(opt->minpp >= 0.0f && opt->minpp < 1.0f)) throw Error(CBP_ERR_ARG, "MINPP must be in [0,1)");
+        if (!(opt->eval >= 0.0f)) throw Error(CBP_ERR_ARG, "EVAL must be >= 0");
         int ndev = 0;
         CBP_CUDA(cudaGetDeviceCount(&ndev));
         if (device < 0 || device >= ndev) throw Error(CBP_ERR_ARG, "invalid device");
@@ -556,7 +561,6 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             a.ssswgt = c->opt.ssswgt;
             a.ddmswgt = c->opt.ddmswgt;
             a.initshift = c->opt.mapaln ? 0.002f : 0.0003f;
-            a.ddmsshift = 0.2f * c->opt.ddmswgt;
             a.dstsegm = c->opt.dstsegm;
             a.sstab = c->sstab.as<float>();
             a.dmstab = c->dmstab.as<float>();

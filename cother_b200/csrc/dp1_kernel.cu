@@ -69,8 +69,24 @@ dp1_kernel(const Dp1Args a)
         const float qDDp = rv ? a.qtrn[trDD * QT + r] : kLog0;
         const float qMIc = rv ? a.qtrn[trMI * QT + r + 1] : kLog0;
         const float qIIc = rv ? a.qtrn[trII * QT + r + 1] : kLog0;
+        // column -1 of row r, as the reference's block schedule leaves it
+        // (src/libmycu/cudp/CuBatchDP_init_btck.cu:93-160, 190-300): its
+        // leftmost block diagonal of each 32-row band starts 32 columns left
+        // of the profile and computes cells there with log-zero profile
+        // transitions and score -9, so MM = 0, MI = IM = ND ~ -32768 and
+        // DN(r) = max(qMD(r), DN(r-1) + qDD(r)), from max(qMD, qDD) on the
+        // band's first row. The band's last row is started by the next
+        // block diagonal at column 0 with zeroed predecessors.
+        float dnv = hmax(0.0f + qMDp, 0.0f + qDDp);
+        for (int k = 1; k < 31; k++) {
+            const float up = __shfl_up_sync(kFull, dnv, 1);
+            if (lane == k) dnv = hmax(0.0f + qMDp, up + qDDp);
+        }
+        const bool lastrow = (lane == 31);
         // this lane's latest cell (r, c-1): the "left" states
-        float lMM = 0.f, lMI = 0.f, lIM = 0.f, lDN = 0.f, lND = 0.f;
+        float lMM = 0.f;
+        float lMI = lastrow ? 0.f : kLog0, lIM = lastrow ? 0.f : kLog0;
+        float lDN = lastrow ? 0.f : dnv, lND = lastrow ? 0.f : kLog0;
         // the previous step's "up" = this step's "diagonal"
         float dMM = 0.f, dMI = 0.f, dIM = 0.f, dDN = 0.f, dND = 0.f;
         const bool top = (r0 == 0);
@@ -90,6 +106,10 @@ dp1_kernel(const Dp1Args a)
                 } else {
                     uMM = uMI = uIM = uDN = uND = 0.f;
                 }
+            }
+            if (lastrow && c == 0) {
+                // the band's last row takes zeroed predecessors at column 0
+                dMM = dMI = dIM = dDN = dND = 0.f;
             }
             if (rv && c >= 0 && c < Ld) {
                 const long long e = tb + c;

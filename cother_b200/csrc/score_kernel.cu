@@ -14,6 +14,7 @@
 // efficiency: byte-packed distance lists in shared memory (odd word stride,
 // conflict-free for lanes in step), a 22x22 pair-score table in shared
 // memory, and one code path for upper and lower diagonals.
+#include <cmath>
 #include "common.cuh"
 #include "cbmath.cuh"
 #include "layout.h"
@@ -288,8 +289,10 @@ score_matrix_kernel(const ScoreArgs a)
                 const float sum = ddms_cell(s_qe + r * kElems, qlen, de, dlen, s_dms, a.dstsegm);
                 const float dm = __fmaf_rn(0.053f * 16.0f, sum, -1.235f) * a.ddmswgt;
                 if (dm != 0.0f) {
+                    // the modular score drops 0.2*DDMSWGT, in the contracted
+                    // form of CuBatchScoreMatrix_ddms2s_h2.cu:171
                     s = s + dm;
-                    mod = mod + (dm - a.ddmsshift);
+                    mod = mod + __fmaf_rn(-0.2f, a.ddmswgt, dm);
                 }
             }
         }
@@ -310,9 +313,12 @@ void launch_score_matrix(const ScoreArgs& a, cudaStream_t stream)
 }
 
 // Pair-score table over packed distance codes (0..20 saturated, 21 = no
-// data), computed on the host with each operation rounded separately, as
-// the reference's own CPU table does (cother-scores-optimizer/dstable.h:339-365,
-// constants src/libmycu/cupro/SerializedDstMatchScoresAttr.h:29-31).
+// data), computed on the host (constants
+// src/libmycu/cupro/SerializedDstMatchScoresAttr.h:29-31, formula
+// src/libmycu/cupro/SerializedDstMatchScores.cuh:347-396). With d1 >= d2 the
+// reference's CUDA build evaluates intercept = 0.35 - (d2*-0.4)*0.05 and
+// score = d1*slope + intercept as two fused multiply-adds (nvcc contracts
+// them by default), so the table does the same with fmaf.
 void build_dms_table(float* T)
 {
     volatile float s00 = 0.35f, s200 = -0.4f, inv = 0.05f;
@@ -321,12 +327,10 @@ void build_dms_table(float* T)
             if (a1 == kDstNoData || a2 == kDstNoData) { T[a1 * kDstCard + a2] = -1.0f; continue; }
             int d1 = a1 > a2 ? a1 : a2, d2 = a1 > a2 ? a2 : a1;
             volatile float t = (float)d2 * s200;
-            volatile float t2 = t * inv;
-            volatile float intpt = s00 - t2;
+            volatile float intpt = std::fmaf(-t, inv, s00);
             volatile float sl0 = s200 - s00;
             volatile float slope = sl0 * inv;
-            volatile float prod = (float)d1 * slope;
-            T[a1 * kDstCard + a2] = prod + intpt;
+            T[a1 * kDstCard + a2] = std::fmaf((float)d1, slope, intpt);
         }
 }
 

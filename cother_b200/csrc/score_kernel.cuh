@@ -13,7 +13,7 @@ struct ScoreArgs {
     int ncols = 0;        // slab positions
     long long ld = 0;     // leading dimension of the outputs
     int Lq = 0;
-    float ssswgt = 0.f, ddmswgt = 0.f, initshift = 0.f, ddmsshift = 0.f;
+    float ssswgt = 0.f, ddmswgt = 0.f, initshift = 0.f;
     int dstsegm = 6;
     const float* sstab = nullptr;   // [30][30]
     const float* dmstab = nullptr;  // [22][22]

@@ -50,20 +50,33 @@ float orc_logf(float x)
  * src/libmycu/cupro/SerializedDstMatchScoresAttr.h:29-31 and
  * SerializedDstMatchScores.cuh:19-20): distances saturate at 20
  * (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:60), 255 scores -1;
- * with d1 >= d2: score = d1*slope + (0.35 - d2*(-0.4)*0.05),
- * slope = (-0.4-0.35)*0.05, each operation rounded separately as in the
- * reference's own CPU table (cother-scores-optimizer/dstable.h:339-365).
+ * with d1 >= d2: score = d1*slope + (0.35 - (d2*(-0.4))*0.05),
+ * slope = (-0.4-0.35)*0.05. The reference's CUDA build contracts both
+ * multiply-adds (nvcc's default --fmad=true): the intercept is
+ * fma(-(d2*-0.4), 0.05, 0.35) and the score fma(d1, slope, intercept),
+ * which its own CPU table (cother-scores-optimizer/dstable.h:339-365)
+ * rounds separately; the GPU form is the one followed here.
  */
-float orc_dms_pair_score(int d1, int d2)
+static float orc_dms_pair_score_ex(int d1, int d2, int fused)
 {
     if (d1 == 0xff || d2 == 0xff) return -1.0f;
     if (d1 > 20) d1 = 20;
     if (d2 > 20) d2 = 20;
     if (d1 < d2) { int t = d1; d1 = d2; d2 = t; }
-    float intpt = 0.35f - ((float)d2 * -0.4f) * 0.05f;
+    float b = (float)d2 * -0.4f;
     float slope = (-0.4f - 0.35f) * 0.05f;
-    float prod = (float)d1 * slope;
-    return prod + intpt;
+    if (!fused) {
+        float intpt = 0.35f - b * 0.05f;
+        float prod = (float)d1 * slope;
+        return prod + intpt;
+    }
+    float intpt = fmaf(-b, 0.05f, 0.35f);
+    return fmaf((float)d1, slope, intpt);
+}
+
+float orc_dms_pair_score(int d1, int d2)
+{
+    return orc_dms_pair_score_ex(d1, d2, 1);
 }
 
 /* ------------------------------------------------------------------------
@@ -124,27 +137,27 @@ static inline int orc_lv(const uint8_t* lst, int k)
     return lst[k];
 }
 
-static inline float orc_S(const uint8_t* q, int kq, const uint8_t* d, int kd)
+static inline float orc_S(const uint8_t* q, int kq, const uint8_t* d, int kd, int fused)
 {
-    return orc_dms_pair_score(orc_lv(q, kq), orc_lv(d, kd));
+    return orc_dms_pair_score_ex(orc_lv(q, kq), orc_lv(d, kd), fused);
 }
 
 /* Upper part: diagonal j of the DP over the two lists
  * (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:288-340, segment
  * update :124-147, unrolled reads :184-198). */
 static void orc_diag_upper(const uint8_t* q, const uint8_t* d, int dstsegm, int len1, int len2,
-                           int j, float* ms, uint32_t* mc)
+                           int j, float* ms, uint32_t* mc, int fused)
 {
     float segsco;
     int segqb = 0, segpb = j;
     float s[5];
-    s[0] = orc_S(q, 1, d, j + 1);
+    s[0] = orc_S(q, 1, d, j + 1, fused);
     segsco = orc_hmax(s[0], 0.0f);
     for (int i = 0; i < len1 && j + i < len2; i += 4) {
         float scom = 0.0f;
         int im = 0, jim = 0, ib = 0, jib = 0;
-        s[2] = orc_S(q, i + 3, d, j + i + 3);
-        s[4] = orc_S(q, i + 5, d, j + i + 5);
+        s[2] = orc_S(q, i + 3, d, j + i + 3, fused);
+        s[4] = orc_S(q, i + 5, d, j + i + 5, fused);
         s[3] = 0.5f * (s[2] + s[4]);
         s[1] = 0.5f * (s[0] + s[2]);
         for (int k = 1; k <= 4; k++) {
@@ -166,18 +179,18 @@ static void orc_diag_upper(const uint8_t* q, const uint8_t* d, int dstsegm, int 
 /* Lower part: diagonal i (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:345-396,
  * segment update :153-176). */
 static void orc_diag_lower(const uint8_t* q, const uint8_t* d, int dstsegm, int len1, int len2,
-                           int i, float* ms, uint32_t* mc)
+                           int i, float* ms, uint32_t* mc, int fused)
 {
     float segsco;
     int segqb = i, segpb = 0;
     float s[5];
-    s[0] = orc_S(q, i + 1, d, 1);
+    s[0] = orc_S(q, i + 1, d, 1, fused);
     segsco = orc_hmax(s[0], 0.0f);
     for (int j = 0; j < len2 && i + j < len1; j += 4) {
         float scom = 0.0f;
         int ijm = 0, jm = 0, ijb = 0, jb = 0;
-        s[2] = orc_S(q, i + j + 3, d, j + 3);
-        s[4] = orc_S(q, i + j + 5, d, j + 5);
+        s[2] = orc_S(q, i + j + 3, d, j + 3, fused);
+        s[4] = orc_S(q, i + j + 5, d, j + 5, fused);
         s[3] = 0.5f * (s[2] + s[4]);
         s[1] = 0.5f * (s[0] + s[2]);
         for (int k = 1; k <= 4; k++) {
@@ -202,6 +215,12 @@ static void orc_diag_lower(const uint8_t* q, const uint8_t* d, int dstsegm, int 
 float orc_ddms_cell(const uint8_t* qlist, const uint8_t* dlist, int dstsegm,
                     float ddmswgt, float* rawsum, int* computed)
 {
+    return orc_ddms_cell_ex(qlist, dlist, dstsegm, ddmswgt, 1, rawsum, computed);
+}
+
+float orc_ddms_cell_ex(const uint8_t* qlist, const uint8_t* dlist, int dstsegm,
+                       float ddmswgt, int fused, float* rawsum, int* computed)
+{
     int len1 = qlist[0], len2 = dlist[0];
     *rawsum = 0.0f;
     *computed = 0;
@@ -210,9 +229,9 @@ float orc_ddms_cell(const uint8_t* qlist, const uint8_t* dlist, int dstsegm,
     float ms[3] = {0.0f, 0.0f, 0.0f};
     uint32_t mc[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
     for (int j = len2 >> 2; 0 <= j; j -= 2)
-        orc_diag_upper(qlist, dlist, dstsegm, len1, len2, j, ms, mc);
+        orc_diag_upper(qlist, dlist, dstsegm, len1, len2, j, ms, mc, fused);
     for (int i = len1 >> 2; 0 < i; i -= 2)
-        orc_diag_lower(qlist, dlist, dstsegm, len1, len2, i, ms, mc);
+        orc_diag_lower(qlist, dlist, dstsegm, len1, len2, i, ms, mc, fused);
     float sum = 0.0f;
     for (int k = 0; k < 3; k++) sum = sum + ms[k];
     *rawsum = sum;
@@ -270,7 +289,6 @@ void orc_score_matrix(int Lq, const float* q_tf, const float* q_bkg, const float
                       long long col0, long long ncols,
                       float* scores, float* modscores, long long ld)
 {
-    const float ddmsshift = 0.2f * prm->ddmswgt;
     for (int r = 0; r < Lq; r++) {
         for (long long c = col0; c < col0 + ncols; c++) {
             int p = d_pro[c];
@@ -287,8 +305,10 @@ void orc_score_matrix(int Lq, const float* q_tf, const float* q_bkg, const float
                                          d_dd + (size_t)c * ORC_NDSTSLOTS,
                                          prm->dstsegm, prm->ddmswgt, &raw, &comp);
                 if (comp && dm != 0.0f) {
+                    /* modular score: dm - 0.2*DDMSWGT, contracted as the
+                     * reference's kernel is (CuBatchScoreMatrix_ddms2s_h2.cu:171) */
                     s = s + dm;
-                    ms = ms + (dm - ddmsshift);
+                    ms = ms + fmaf(-0.2f, prm->ddmswgt, dm);
                 }
             }
             scores[(size_t)r * ld + (c - col0)] = s;
@@ -351,6 +371,8 @@ void orc_score_matrix_mt(int nthreads, int Lq, const float* q_tf, const float* q
  */
 enum { ORC_MM = 0, ORC_MI, ORC_MD, ORC_IM, ORC_II, ORC_DM, ORC_DD };
 enum { ORC_STOP = 0, ORC_LEFT = 1, ORC_UP = 2, ORC_DIAG = 3 };
+/* log of zero probability in the reference's DP (CuBatchDP_init.cuh:35-38) */
+#define ORC_LOG0 (-32768.0f)
 
 static int orc_corner_edge(int Lq, int Ld)
 {
@@ -380,12 +402,34 @@ float orc_dp1_profile(int Lq, int Ld, const float* S, long long lds,
 #define PIM(a, c) a[2 * w + (c)]
 #define PDN(a, c) a[3 * w + (c)]
 #define PND(a, c) a[4 * w + (c)]
+    float dnv = 0.0f;   /* DN of the column -1 cell of the previous row */
     for (int r = 0; r < Lq; r++) {
         const float qMMp = qtrn[ORC_MM * qts + r], qIMp = qtrn[ORC_IM * qts + r];
         const float qDMp = qtrn[ORC_DM * qts + r], qMDp = qtrn[ORC_MD * qts + r];
         const float qDDp = qtrn[ORC_DD * qts + r];
         const float qMIc = qtrn[ORC_MI * qts + r + 1], qIIc = qtrn[ORC_II * qts + r + 1];
-        for (int k = 0; k < 5; k++) cur[k * w] = 0.0f;
+        /* column -1 (left boundary), as the reference's block schedule
+         * leaves it (src/libmycu/cudp/CuBatchDP_init_btck.cu:93-160,
+         * 190-300): within each band of 32 rows, the leftmost block
+         * diagonal starts 32 columns left of the profile, and its threads
+         * there compute cells with log-zero profile transitions
+         * (CuBatchDP_init.cuh:35-38, -32768) and score -9: MM = 0,
+         * MI = IM = ND ~ -32768, DN = max(qMD(r), DN(r-1) + qDD(r)) from
+         * max(qMD, qDD) on the band's first row (zeros above it). The
+         * band's last row starts the next block diagonal at column 0 with
+         * zero-initialised predecessors, and the first row's diagonal
+         * predecessor lies in the zeroed bottom cache. */
+        if ((r & 31) == 31) {
+            for (int k = 0; k < 5; k++) { cur[k * w] = 0.0f; prv[k * w] = 0.0f; }
+        } else {
+            float up_dn = ((r & 31) == 0) ? 0.0f : dnv;
+            dnv = orc_hmax(0.0f + qMDp, up_dn + qDDp);
+            cur[0 * w] = 0.0f;
+            cur[1 * w] = ORC_LOG0;
+            cur[2 * w] = ORC_LOG0;
+            cur[3 * w] = dnv;
+            cur[4 * w] = ORC_LOG0;
+        }
         for (int c = 0; c < Ld; c++) {
             const float dMMp = dtrn[ORC_MM * dts + c], dIMp = dtrn[ORC_IM * dts + c];
             const float dDMp = dtrn[ORC_DM * dts + c], dMDp = dtrn[ORC_MD * dts + c];

@@ -10,6 +10,13 @@
  * FP32 in the reference's operation order; multiply-adds that the reference
  * compiler contracts are written as fmaf(), and the file is compiled with
  * -ffp-contract=off so no other contraction happens.
+ *
+ * Pinned against the reference's own code: its CUDA kernels, compiled from
+ * their sources (Makefile target refgpu) and run on a B200 by
+ * tests/golden/make_ref_gpu_fixtures.py, give the golden files
+ * tests/golden/ref_gpu_*.npz that tests/test_ref_gpu_pin.py checks every
+ * stage against; the DDMS is also checked against the reference's CPU
+ * restatement (cother-scores-optimizer/ddms.cxx, target ref).
  */
 #ifndef COTHER_ORACLE_H
 #define COTHER_ORACLE_H
@@ -44,6 +51,12 @@ float orc_dms_pair_score(int d1, int d2);
  * *computed is 0 when a list is shorter than dstsegm */
 float orc_ddms_cell(const uint8_t* qlist, const uint8_t* dlist, int dstsegm,
                     float ddmswgt, float* rawsum, int* computed);
+
+/* The same with the pair-score rounding chosen: fused = 1 is the reference's
+ * CUDA kernel (two fused multiply-adds), fused = 0 its CPU restatement in
+ * cother-scores-optimizer/dstable.h (each operation rounded). */
+float orc_ddms_cell_ex(const uint8_t* qlist, const uint8_t* dlist, int dstsegm,
+                       float ddmswgt, int fused, float* rawsum, int* computed);
 
 /* Score matrices for one query against N database positions.
  *   q_tf [20][Lq], q_bkg [20], q_ss [3][Lq], q_dd [Lq][100] (uint8)

@@ -22,14 +22,16 @@ _ref = None
 
 
 def build(force: bool = False) -> None:
-    """Compile the oracle (and the reference DDMS restatement when the
-    reference tree is present)."""
+    """Compile the oracle and, when the reference tree is present, the
+    reference's DDMS restatement and its CUDA kernels (oracle/_ref/)."""
     args = ["make", "-s", "-C", HERE, "all"]
     if force:
         subprocess.run(["make", "-s", "-C", HERE, "clean"], check=True)
     subprocess.run(args, check=True)
     if os.path.isdir(os.path.join(REFERENCE_TREE, "cother-scores-optimizer")):
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if os.path.isdir(os.path.join(REFERENCE_TREE, "src", "libmycu")):
+        subprocess.run(["make", "-s", "-C", HERE, "refgpu"], check=True)
 
 
 def lib():
@@ -45,6 +47,11 @@ def lib():
         L.orc_ddms_cell.restype = ctypes.c_float
         L.orc_ddms_cell.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float,
                                     ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]
+        L.orc_ddms_cell_ex.restype = ctypes.c_float
+        L.orc_ddms_cell_ex.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.c_float, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_float),
+                                       ctypes.POINTER(ctypes.c_int)]
         sm_args = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                    ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -94,13 +101,17 @@ def logf(x: float) -> float:
     return lib().orc_logf(x)
 
 
-def ddms_cell(qlist: np.ndarray, dlist: np.ndarray, dstsegm: int = 6, ddmswgt: float = 0.2):
+def ddms_cell(qlist: np.ndarray, dlist: np.ndarray, dstsegm: int = 6, ddmswgt: float = 0.2,
+              fused: bool = True):
+    """DDMS of one cell: (score, top-3 sum, computed). `fused` selects the
+    pair-score rounding of the reference's CUDA kernel (True) or of its CPU
+    restatement in cother-scores-optimizer (False)."""
     q = np.ascontiguousarray(qlist, dtype=np.uint8)
     d = np.ascontiguousarray(dlist, dtype=np.uint8)
     raw = ctypes.c_float()
     comp = ctypes.c_int()
-    s = lib().orc_ddms_cell(q.ctypes.data, d.ctypes.data, dstsegm, ddmswgt,
-                            ctypes.byref(raw), ctypes.byref(comp))
+    s = lib().orc_ddms_cell_ex(q.ctypes.data, d.ctypes.data, dstsegm, ddmswgt, int(fused),
+                               ctypes.byref(raw), ctypes.byref(comp))
     return s, raw.value, comp.value
 
 

@@ -5,7 +5,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+from conftest import GOLDEN, ROOT
 
 
 def test_logf_accuracy(oracle_lib):
@@ -33,11 +33,12 @@ def test_dms_pair_scores(oracle_lib):
 
 def test_ddms_matches_reference_cpu_code(oracle_lib):
     """The oracle's DDMS segment DP equals the reference's own CPU
-    restatement (cother-scores-optimizer/ddms.cxx) on committed vectors."""
+    restatement (cother-scores-optimizer/ddms.cxx) on committed vectors, with
+    that restatement's pair-score rounding (each operation rounded)."""
     z = np.load(os.path.join(GOLDEN, "ddms_ref.npz"))
     n = 0
     for q, d, r in zip(z["qlists"], z["dlists"], z["ref"]):
-        s, raw, comp = oracle_lib.ddms_cell(q, d)
+        s, raw, comp = oracle_lib.ddms_cell(q, d, fused=False)
         if r == -777.0:
             continue
         assert comp == 1
@@ -57,7 +58,7 @@ def test_ddms_matches_reference_live(oracle_lib):
     ql, dl = q.dd_lists(), d.dd_lists()
     for i in range(0, 70, 3):
         for j in range(0, 120, 7):
-            s, raw, comp = oracle_lib.ddms_cell(ql[i], dl[j])
+            s, raw, comp = oracle_lib.ddms_cell(ql[i], dl[j], fused=False)
             x = np.full(110, 255, np.int32); x[:ql[i][0] + 1] = ql[i][:ql[i][0] + 1]
             y = np.full(110, 255, np.int32); y[:dl[j][0] + 1] = dl[j][:dl[j][0] + 1]
             r = R.ref_ddms_scaled_sum(x.ctypes.data, y.ctypes.data)
@@ -85,3 +86,18 @@ def test_score_matrix_oracle_shapes(oracle_lib, ss_table):
     assert np.isfinite(sc).all() and np.isfinite(ms).all()
     sc2, ms2 = oracle_lib.score_matrix(q, db, ss_table, col0=17, ncols=40, nthreads=3)
     assert np.array_equal(sc2, sc[:, 17:57]) and np.array_equal(ms2, ms[:, 17:57])
+
+
+def test_library_nn_weights_equal_fixture():
+    """The significance-network weights compiled into the CUDA library
+    (kNNWeightsTable in cother_b200/csrc/api.cu) are the reference's table
+    (src/libmycu/cupro/CuDeviceMemory.cu:43-80, fixture nn_weights.npy)."""
+    import re
+    src = open(os.path.join(ROOT, "cother_b200", "csrc", "api.cu")).read()
+    i = src.index("kNNWeightsTable[kNNWeights] = {")
+    body = src[i:src.index("};", i)].split("{", 1)[1]
+    vals = np.array([np.float32(v.rstrip("f")) for v in
+                     re.findall(r"[-+]?[0-9]*\.?[0-9]+(?:[eE][-+]?[0-9]+)?f?", body)], np.float32)
+    ref = np.load(os.path.join(GOLDEN, "nn_weights.npy"))
+    assert vals.shape == ref.shape
+    assert np.array_equal(vals, ref)

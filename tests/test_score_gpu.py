@@ -55,12 +55,13 @@ def test_score_matrix_last_slab(oracle_lib, ss_table):
 
 
 def test_score_matrix_options(oracle_lib, ss_table):
-    """DDMS off, other weights, DSTSEGM and MAPALN=0 shift."""
+    """DDMS off, SS off, other weights, DSTSEGM and MAPALN=0 shift."""
     from cother_b200 import synth
     q = synth.make_profiles([21], 41, True)
     db = synth.make_profiles([33, 18], 42, False)
     for opt, orc in [
         (dict(ddmswgt=0.0), dict(ddmswgt=0.0)),
+        (dict(ssswgt=0.0), dict(ssswgt=0.0)),
         (dict(ssswgt=0.3, ddmswgt=0.5, dstsegm=3), dict(ssswgt=0.3, ddmswgt=0.5, dstsegm=3)),
         (dict(mapaln=0), dict(initshift=0.0003)),
     ]:
