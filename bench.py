@@ -250,6 +250,7 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     kern_ms, launches = 0.0, 0
     score_ms, score_launches = 0.0, 0
+    stage_acc = [0.0] * len(STAGES)
     e0.record(stream)
     d2h = 0
     nhits = 0
@@ -260,6 +261,7 @@ def main():
         d2h = recs.nbytes + rows.nbytes
         nhits = len(recs)
         st = bp.stage_times()
+        stage_acc = [a + b for a, b in zip(stage_acc, st)]
         kern_ms += sum(st)
         score_ms += st[0]
         launches += bp.launch_count()
@@ -303,6 +305,7 @@ def main():
                         "h2d_bytes_per_step": int(Lq * (4 * 20 + 4 * 3 + 4 * 100 + 2) + 4 * 7 * (Lq + 1)),
                         "d2h_bytes_per_step": int(d2h)},
                 "hits": nhits,
+                "stage_ms": {k: v / steps for k, v in zip(STAGES, stage_acc)},
                 "gpu_launches": launches, "roofline": roof, "clocks": clocks}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds, db_len, nseqs)

@@ -32,33 +32,57 @@ constexpr int kElems = 104;        // list elements held per position (99 + over
 constexpr int kDbStride = 108;     // bytes per database list in shared memory (27 words)
 
 // Top-3 register of non-intersecting segments
-// (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s.cuh:182-251). Coordinates
-// are packed [QB QE PB PE]; two segments intersect when their query OR
-// their database ranges overlap (ddms2s.cuh:162-173).
-__device__ __forceinline__ bool coords_intersect(uint32_t c1, uint32_t c2)
+// (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s.cuh:182-251). The reference
+// packs a segment's coordinates into one word [QB QE PB PE] and tests
+// intersection with per-byte SIMD min/max. Here a segment is two words,
+// begins (QB<<16 | PB) and ends (QE<<16 | PE), so that the test uses the
+// native halfword SIMD min/max of sm_90+: two segments intersect when their
+// query OR their database ranges overlap (ddms2s.cuh:162-173), i.e. when
+// min(end) >= max(begin) in either halfword; adding 256 to each halfword
+// before subtracting keeps both non-negative (positions < 256), so the test
+// is whether bits 8..15 of either half are set. The coordinates of an empty
+// entry (score 0) are never consulted for a decision, as in the reference.
+__device__ __forceinline__ uint32_t vmax_u16x2(uint32_t a, uint32_t b)
 {
-    uint32_t mx = __vmaxu4(c1, c2);
-    uint32_t mn = __vminu4(c1, c2);
-    return ((mn >> 16) & 0xffu) >= ((mx >> 24) & 0xffu) || (mn & 0xffu) >= ((mx >> 8) & 0xffu);
+    uint32_t r;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
 }
-
-__device__ __forceinline__ void register_max(float (&ms)[3], uint32_t (&mc)[3], float s, uint32_t c)
+__device__ __forceinline__ uint32_t vmin_u16x2(uint32_t a, uint32_t b)
 {
+    uint32_t r;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ bool seg_intersect(uint32_t b1, uint32_t e1, uint32_t b2, uint32_t e2)
+{
+    const uint32_t mx = vmax_u16x2(b1, b2), mn = vmin_u16x2(e1, e2);
+    return ((mn + 0x01000100u - mx) & 0xff00ff00u) != 0u;
+}
+__device__ __forceinline__ void register_max(float (&ms)[3], uint32_t (&mb)[3], uint32_t (&me)[3],
+                                             float s, uint32_t cb, uint32_t ce)
+{
+    // every case of the reference's register tests the candidate against
+    // the entries at ranks 0 and 1 (an empty entry's test never matters)
+    const bool x0 = seg_intersect(cb, ce, mb[0], me[0]);
+    const bool x1 = seg_intersect(cb, ce, mb[1], me[1]);
     if (ms[0] <= s) {
-        ms[2] = ms[1]; mc[2] = mc[1];
-        ms[1] = ms[0]; mc[1] = mc[0];
-        ms[0] = s; mc[0] = c;
-        if (ms[1] != 0.0f && coords_intersect(mc[0], mc[1])) ms[1] = 0.0f;
-        if (ms[2] != 0.0f && coords_intersect(mc[0], mc[2])) ms[2] = 0.0f;
-        if (ms[1] == 0.0f) { ms[1] = ms[2]; mc[1] = mc[2]; ms[2] = 0.0f; }
+        const float a1 = x0 ? 0.0f : ms[0];
+        const float a2 = x1 ? 0.0f : ms[1];
+        const bool up = (a1 == 0.0f);
+        ms[2] = up ? 0.0f : a2;
+        ms[1] = up ? a2 : a1;
+        const uint32_t b1 = up ? mb[1] : mb[0], e1 = up ? me[1] : me[0];
+        mb[2] = mb[1]; me[2] = me[1];
+        mb[1] = b1; me[1] = e1;
+        ms[0] = s; mb[0] = cb; me[0] = ce;
     } else if (ms[1] <= s) {
-        if (coords_intersect(c, mc[0])) return;
-        ms[2] = ms[1]; mc[2] = mc[1];
-        ms[1] = s; mc[1] = c;
-        if (coords_intersect(mc[1], mc[2])) ms[2] = 0.0f;
+        if (!x0) {
+            ms[2] = x1 ? 0.0f : ms[1]; mb[2] = mb[1]; me[2] = me[1];
+            ms[1] = s; mb[1] = cb; me[1] = ce;
+        }
     } else if (ms[2] <= s) {
-        if (coords_intersect(c, mc[0]) || coords_intersect(c, mc[1])) return;
-        ms[2] = s; mc[2] = c;
+        if (!x0 && !x1) { ms[2] = s; mb[2] = cb; me[2] = ce; }
     }
 }
 
@@ -97,13 +121,13 @@ __device__ __forceinline__ float sat_mul(float a, float b)
 __device__ __forceinline__ void ddms_diagonal(
     const uint8_t* __restrict__ q, const uint8_t* __restrict__ d,
     const float* __restrict__ T, int lim, int oq, int od, float nsegm1,
-    float (&ms)[3], uint32_t (&mc)[3])
+    float (&ms)[3], uint32_t (&mb)[3], uint32_t (&me)[3])
 {
     constexpr float kBig = 0x1p100f;
     float s0 = T[q[0] * kDstCard + d[0]];
     float t = sat_add(s0, 0.0f);
     float ls = 1.0f;
-    const uint32_t cbase = ((uint32_t)oq << 24) | ((uint32_t)oq << 16) | ((uint32_t)od << 8) | (uint32_t)od;
+    const uint32_t cbase = ((uint32_t)oq << 16) | (uint32_t)od;
     for (int x = 0; x < lim; x += 4) {
         const float s2 = T[q[x + 2] * kDstCard + d[x + 2]];
         const float s4 = T[q[x + 4] * kDstCard + d[x + 4]];
@@ -122,17 +146,14 @@ __device__ __forceinline__ void ddms_diagonal(
         const float v3 = t3 * sat_add(l3, nsegm1);
         const float v4 = t4 * sat_add(l4, nsegm1);
         const float scom = fmaxf(fmaxf(v1, v2), fmaxf(v3, v4));
-        if (scom != 0.0f) {
-            int k;
-            float lk;
-            if (v1 == scom) { k = 1; lk = l1; }
-            else if (v2 == scom) { k = 2; lk = l2; }
-            else if (v3 == scom) { k = 3; lk = l3; }
-            else { k = 4; lk = l4; }
+        // the register is sorted by score, so a candidate below its third
+        // entry changes nothing (every branch of register_max fails)
+        if (scom != 0.0f && ms[2] <= scom) {
+            const int k = (v1 == scom) ? 1 : (v2 == scom) ? 2 : (v3 == scom) ? 3 : 4;
+            const float lk = (v1 == scom) ? l1 : (v2 == scom) ? l2 : (v3 == scom) ? l3 : l4;
             const uint32_t be = (uint32_t)(x + k);
             const uint32_t bb = be + 1u - (uint32_t)lk;
-            const uint32_t c = cbase + ((bb << 24) | (be << 16) | (bb << 8) | be);
-            register_max(ms, mc, scom, c);
+            register_max(ms, mb, me, scom, cbase + bb * 0x00010001u, cbase + be * 0x00010001u);
         }
         s0 = s4;
         t = t4;
@@ -147,12 +168,13 @@ __device__ __forceinline__ float ddms_cell(const uint8_t* __restrict__ q, int le
                                            const float* __restrict__ T, int dstsegm)
 {
     float ms[3] = {0.0f, 0.0f, 0.0f};
-    uint32_t mc[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
+    uint32_t mb[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
+    uint32_t me[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
     const float nsegm1 = -(float)(dstsegm - 1);
     for (int j = len2 >> 2; 0 <= j; j -= 2)
-        ddms_diagonal(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mc);
+        ddms_diagonal(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mb, me);
     for (int i = len1 >> 2; 0 < i; i -= 2)
-        ddms_diagonal(q + i, d, T, min(len2, len1 - i), i, 0, nsegm1, ms, mc);
+        ddms_diagonal(q + i, d, T, min(len2, len1 - i), i, 0, nsegm1, ms, mb, me);
     float sum = 0.0f;
     sum = sum + ms[0];
     sum = sum + ms[1];

@@ -102,6 +102,18 @@ unsigned blocks_per_diagonal(size_t dblen, size_t qlen, size_t w, size_t b)
     return (unsigned)(along_q < along_d ? along_q : along_d);
 }
 
+struct Events {
+    cudaEvent_t e[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    Events()
+    {
+        for (auto& x : e) ck(cudaEventCreate(&x), "event");
+    }
+    ~Events()
+    {
+        for (auto& x : e) if (x) cudaEventDestroy(x);
+    }
+};
+
 struct DevBuf {
     char* p = nullptr;
     ~DevBuf() { if (p) cudaFree(p); }
@@ -154,6 +166,12 @@ typedef struct refgpu_job {
     unsigned int globvars[4];  // passed profiles, their positions, max length
     int dblen;
     size_t dbalnlen2;
+    // timing: with copy_matrices = 0 the score matrices and backtrack codes
+    // stay on the device (their pointers may be null); stage_ms receives the
+    // device time of the score matrix, phase 1 (DP + finalization),
+    // statistics and MAP, measured with events around each stage's launches
+    int copy_matrices;
+    float stage_ms[4];
 } refgpu_job;
 
 int refgpu_run(refgpu_job* J)
@@ -168,6 +186,13 @@ int refgpu_run(refgpu_job* J)
         J->dblen = (int)dblen;
         if (Lq < 1 || N < 1 || P < 1)
             throw Fail{"empty query or database"};
+        // the reference's kernels index a chunk's cells with 32-bit ints
+        // ((y-i)*dblen + i, CuBatchDP_init_btck.cu:488); its memory planner
+        // keeps chunks below INT_MAX/Lq positions
+        // (CuDeviceMemory.cuh:658-690), and so must the caller
+        if ((double)Lq * (double)(dblen + 64) >= 2147483647.0)
+            throw Fail{"chunk too large for the reference's 32-bit cell indices: "
+                       "split the database"};
         // the statistics kernels' stack size is not known statically: give
         // every thread a generous stack; the dynamic launches per passed pair
         // (a parent and six children) stay well under the pending-launch limit
@@ -269,6 +294,10 @@ int refgpu_run(refgpu_job* J)
 
         const bool modinuse = J->ssswgt > 0.0f;   // CVSWGT is 0 here
         const uint nq = (uint)Lq, n1 = 0, nC = (uint)N, pad = (uint)dbxpad;
+        Events ev;
+        for (float& t : J->stage_ms) t = 0.0f;
+        ck(cudaDeviceSynchronize(), "setup");
+        ck(cudaEventRecord(ev.e[0]), "event");
 
         // --- score matrix
         dim3 sthr(SMINIT_2DCACHE_DIM, SMINIT_2DCACHE_DIM, 1);
@@ -288,11 +317,15 @@ int refgpu_run(refgpu_job* J)
                                                    nq, n1, nC, pad, 0, 0, 0, scores, modscores);
             ck_launch("DDMS scores");
         }
+        ck(cudaEventRecord(ev.e[1]), "event");
         ck(cudaDeviceSynchronize(), "score matrix");
-        ck(cudaMemcpy(J->scores, scores, Lq * dblen * sizeof(float), cudaMemcpyDeviceToHost),
-           "scores");
-        ck(cudaMemcpy(J->modscores, modscores, Lq * dblen * sizeof(float),
-                      cudaMemcpyDeviceToHost), "modscores");
+        ck(cudaEventElapsedTime(&J->stage_ms[0], ev.e[0], ev.e[1]), "event time");
+        if (J->copy_matrices) {
+            ck(cudaMemcpy(J->scores, scores, Lq * dblen * sizeof(float), cudaMemcpyDeviceToHost),
+               "scores");
+            ck(cudaMemcpy(J->modscores, modscores, Lq * dblen * sizeof(float),
+                          cudaMemcpyDeviceToHost), "modscores");
+        }
 
         // --- phase-1 DP over block diagonals
         {
@@ -309,17 +342,20 @@ int refgpu_run(refgpu_job* J)
             uint nintdivs = (uint)(Lq - 1) / w;
             float nsepds = (float)CUDP_2DCACHE_DIM_D / (float)CUDP_2DCACHE_DIM_X + 1.0f;
             uint lastdiag = (uint)(nsepds * (float)nintdivs) + 1 - 1;
+            ck(cudaEventRecord(ev.e[1]), "event");
             for (uint dd = 0; dd < nblkdiags; dd++) {
                 ExecDP_Btck_Unroll32x<<<blk, thr>>>(dd, lastdiag, 0, 0, 0, 0, nq, n1, nC, pad,
                                                      0, 0, 0, scores, diag, bot, maxc, btck);
                 ck_launch("phase-1 DP");
             }
-            ck(cudaDeviceSynchronize(), "phase-1 DP");
-            ck(cudaMemcpy(J->btck, btck, Lq * dblen, cudaMemcpyDeviceToHost), "btck");
             FinalizeDP<<<1, 1>>>(J->scorethld, 0, (uint)P, 0, 0, n1, nC, pad, 0, 0, scores,
                                  diag, bot, maxc, (char*)btck, glob);
             ck_launch("FinalizeDP");
-            ck(cudaDeviceSynchronize(), "FinalizeDP");
+            ck(cudaEventRecord(ev.e[2]), "event");
+            ck(cudaDeviceSynchronize(), "phase 1");
+            ck(cudaEventElapsedTime(&J->stage_ms[1], ev.e[1], ev.e[2]), "event time");
+            if (J->copy_matrices)
+                ck(cudaMemcpy(J->btck, btck, Lq * dblen, cudaMemcpyDeviceToHost), "btck");
             ck(cudaMemcpy(J->phase1, diag, P * nTDP2OutputPhase1 * sizeof(float),
                           cudaMemcpyDeviceToHost), "phase-1 records");
             ck(cudaMemcpy(J->globvars, glob, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost),
@@ -338,12 +374,15 @@ int refgpu_run(refgpu_job* J)
         // --- statistics
         float* ss2 = (float*)(H + oDP2FwdEnd);
         float* alndat = (float*)(H + oSS2End);
+        ck(cudaEventRecord(ev.e[2]), "event");
         CalcStatisticsDynPlm<<<(unsigned)npass, 1>>>(
             J->xuninf != 0, 0, 0, 0, nq, n1, nC, pad, 0, 0, 0, J->ssemodel, J->qyeno,
             J->searchspace, J->reflambda, J->refK, J->explambda, J->expK, scores,
             (float*)(H + oR), ss2, alndat);
         ck_launch("statistics");
+        ck(cudaEventRecord(ev.e[3]), "event");
         ck(cudaDeviceSynchronize(), "statistics");
+        ck(cudaEventElapsedTime(&J->stage_ms[2], ev.e[2], ev.e[3]), "event time");
         ck(cudaMemcpy(J->stats, alndat, npass * nTDP2OutputAlnData * sizeof(float),
                       cudaMemcpyDeviceToHost), "statistics records");
 
@@ -374,6 +413,7 @@ int refgpu_run(refgpu_job* J)
             uint nintdivs = (uint)((Lq - 1) / w);
             float nsepds = (float)CUMAPDP_2DCACHE_DIM_D / (float)CUMAPDP_2DCACHE_DIM_X + 1.0f;
             uint lastdiag = (uint)(nsepds * (float)nintdivs) + 1 - 1;
+            ck(cudaEventRecord(ev.e[3]), "event");
             for (uint dd = 0; dd < nblkdiags; dd++) {
                 ExecMAPDP_Fwd_Unroll32x<<<blk, thr>>>(
                     dd, lastdiag, J->logevthld, modinuse, 0, 0, 0, 0, nq, n1, nC, pad, 0, 0, 0,
@@ -396,7 +436,9 @@ int refgpu_run(refgpu_job* J)
                 J->ssswgt > 0.0f, J->logevthld, 0, 0, 0, 0, nq, n1, nC, pad, 0, 0, 0, dblen2,
                 (uint)dbxpad2, (uint)dbalnlen2, scores, diag, maxc, btck, alndat, outalns);
             ck_launch("MAP finalize");
+            ck(cudaEventRecord(ev.e[4]), "event");
             ck(cudaDeviceSynchronize(), "MAP");
+            ck(cudaEventElapsedTime(&J->stage_ms[3], ev.e[3], ev.e[4]), "event time");
             ck(cudaMemcpy(J->final_recs, alndat, npass * nTDP2OutputAlnData * sizeof(float),
                           cudaMemcpyDeviceToHost), "final records");
             for (int r = 0; r < nTDP2OutputAlignmentSSS; r++)

@@ -108,6 +108,7 @@ class Job(ctypes.Structure):
         ("phase1", ctypes.c_void_p), ("stats", ctypes.c_void_p), ("final_recs", ctypes.c_void_p),
         ("alns", ctypes.c_void_p), ("alns_cap", ctypes.c_size_t),
         ("globvars", ctypes.c_uint * 4), ("dblen", ctypes.c_int), ("dbalnlen2", ctypes.c_size_t),
+        ("copy_matrices", ctypes.c_int), ("stage_ms", ctypes.c_float * 4),
     ]
 
 
@@ -149,6 +150,7 @@ def run_case(L, q, db, opts):
     j.scores, j.modscores, j.btck = sc.ctypes.data, ms.ctypes.data, bt.ctypes.data
     j.phase1, j.stats, j.final_recs = ph1.ctypes.data, st.ctypes.data, fin.ctypes.data
     j.alns, j.alns_cap = alns.ctypes.data, cap
+    j.copy_matrices = 1
     rc = L.refgpu_run(ctypes.byref(j))
     if rc != 0:
         raise RuntimeError(L.refgpu_error().decode())
