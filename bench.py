@@ -32,6 +32,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 DEFAULT_WORKLOAD = "q400_db50k"
+# DRAM bytes (read + write) per cell of one score_matrix_kernel launch,
+# measured by ncu on q400 x 2,000 profiles (4.29 GB for 195.0 M cells:
+# 8 B/cell of score writes plus the database lists re-read by each 16-row
+# block); the traffic grows with the cells
+SCORE_DRAM_BYTES_PER_CELL = 22.01
 STAGES = ["score_matrix", "phase1_dp", "phase1_finalize", "statistics", "map_realignment"]
 OPS_PER_DDMS_STEP = 50  # algorithmic ops of one 4-cell DDMS step (2 pair scores,
                         # 2 interpolations, 4 segment updates, 1 top-3 register)
@@ -288,7 +293,11 @@ def main():
         sm_mhz = clocks.get("sm_max_mhz") or 1965.0
         alu_peak = 148 * 128 * sm_mhz * 1e6 / 1e9  # lane-ops/s at max clock, Gop/s
         roof = {"bound": "alu", "achieved": achieved, "peak": alu_peak, "unit": "Gop/s",
-                "frac": achieved / alu_peak, "traffic": None,
+                "frac": achieved / alu_peak,
+                "traffic": SCORE_DRAM_BYTES_PER_CELL * float(Lq) * Ndb,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                  "score_matrix_kernel launch at q400 x 2,000 profiles, "
+                                  "scaled by cells (profiles/score_matrix_kernel_q400_db2k.md)",
                 "kernel": "score_matrix_kernel",
                 "peak_source": "148 SMs x 128 FP32 lanes x max SM clock (nominal issue rate)",
                 "hbm_bytes_per_launch": float(Lq) * Ndb * 8,
