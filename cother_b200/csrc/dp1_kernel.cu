@@ -37,12 +37,69 @@ __device__ __forceinline__ bool in_corner(int Lq, int Ld, int edge, int r, int c
     return (Lq <= r + edge && c <= edge + r - Lq) || (Ld - edge + r <= c && r < edge);
 }
 
-__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+// Score tiles and backtrack codes are staged through shared memory so that
+// every global access is a row segment: a band's columns are taken in
+// chunks of 32; chunk k+1's 32x32 score tile is fetched with cp.async while
+// the warp sweeps chunk k (a ring of three tiles: step s touches columns
+// s-31..s), and chunk k's backtrack codes are written back row by row once
+// lane 31 has passed the chunk. Row-major [row][32] tiles are free of bank
+// conflicts both for the row-wise fill (lane t writes column t) and for the
+// anti-diagonal reads (lane t reads row t, column s-t: bank (s-t) mod 32);
+// so are the byte tiles of backtrack codes (bank 8*(t mod 4) + a distinct
+// quarter-column per lane).
+constexpr int kDpWarps = 2;             // warps (profiles) per block
+constexpr int kChunk = 32;              // columns per staged chunk
+constexpr int kScoreRing = 3;           // score tiles in flight per warp
+constexpr int kBtckRing = 2;            // backtrack tiles per warp
+
+struct DpStage {
+    float sc[kScoreRing][32][kChunk];
+    uint8_t bt[kBtckRing][32][kChunk];
+};
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? 4 : 0;   // 0: fill with zeros, read nothing
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// issue the loads of score chunk k of rows r0..r0+31 (zero outside the matrix)
+__device__ __forceinline__ void fetch_chunk(DpStage& st, const float* __restrict__ S, long long ld,
+                                            int r0, int Lq, int Ld, int k, int lane)
+{
+    const int c = k * kChunk + lane;
+    const bool cv = c < Ld;
+    float (*tile)[kChunk] = st.sc[k % kScoreRing];
+#pragma unroll 4
+    for (int i = 0; i < 32; i++) {
+        const bool v = cv && (r0 + i < Lq);
+        const float* src = v ? S + (long long)(r0 + i) * ld + c : S;
+        cp_async4(&tile[i][lane], src, v);
+    }
+}
+
+// write back the backtrack codes of chunk k of rows r0..r0+31
+__device__ __forceinline__ void store_btck_chunk(const DpStage& st, uint8_t* __restrict__ B, long long ld,
+                                                 int r0, int Lq, int Ld, int k, int lane)
+{
+    const int c = k * kChunk + lane;
+    if (c >= Ld) return;
+    const uint8_t (*tile)[kChunk] = st.bt[k % kBtckRing];
+    const int nr = min(32, Lq - r0);
+    for (int i = 0; i < nr; i++) B[(long long)(r0 + i) * ld + c] = tile[i][lane];
+}
+
+__global__ void __launch_bounds__(32 * kDpWarps)
 dp1_kernel(const Dp1Args a)
 {
+    __shared__ DpStage s_stage[kDpWarps];
     const int lane = threadIdx.x & 31;
-    const int pl = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    const int pl = blockIdx.x * kDpWarps + (threadIdx.x >> 5);
     if (pl >= a.nprof) return;  // whole warp
+    DpStage& st = s_stage[threadIdx.x >> 5];
     const int p = a.p0 + pl;
     const int Ld = a.db.plen[p];
     const long long colb = a.db.pstart[p] - a.col0;
@@ -54,6 +111,7 @@ dp1_kernel(const Dp1Args a)
     uint8_t* __restrict__ B = a.btck + colb;
     float* __restrict__ strip = a.bandbuf + colb;  // [5][ld] rows, this profile's columns
     const long long ld = a.ld;
+    const int nchunks = (Ld + kChunk - 1) / kChunk;
 
     float best = 0.0f;
     int bestr = 0, bestc = 0;
@@ -91,7 +149,22 @@ dp1_kernel(const Dp1Args a)
         float dMM = 0.f, dMI = 0.f, dIM = 0.f, dDN = 0.f, dND = 0.f;
         const bool top = (r0 == 0);
         const int nsteps = Ld + 31;
+        __syncwarp();   // the previous band's tiles are no longer read
+        fetch_chunk(st, S, ld, r0, Lq, Ld, 0, lane);
+        cp_async_commit();
         for (int s = 0; s < nsteps; s++) {
+            if ((s & 31) == 0) {
+                // chunk s/32 must be resident; fetch the next one
+                if ((s >> 5) + 1 < nchunks) fetch_chunk(st, S, ld, r0, Lq, Ld, (s >> 5) + 1, lane);
+                cp_async_commit();
+                cp_async_wait1();
+                __syncwarp();
+            } else if ((s & 31) == 31 && s >= 63) {
+                // lane 31 passed chunk (s-63)/32 at the previous step
+                __syncwarp();
+                store_btck_chunk(st, B, ld, r0, Lq, Ld, (s - 63) >> 5, lane);
+                __syncwarp();
+            }
             const int c = s - lane;
             // states of (r-1, c): from lane-1's latest cell, or the strip
             float uMM = __shfl_up_sync(kFull, lMM, 1);
@@ -117,7 +190,8 @@ dp1_kernel(const Dp1Args a)
                 const float dDMp = a.db.trn[trDM * NT + e], dMDp = a.db.trn[trMD * NT + e];
                 const float dDDp = a.db.trn[trDD * NT + e];
                 const float dMIc = a.db.trn[trMI * NT + e + 1], dIIc = a.db.trn[trII * NT + e + 1];
-                const float sc = in_corner(Lq, Ld, edge, r, c) ? -9.0f : S[(long long)r * ld + c];
+                const float sc = in_corner(Lq, Ld, edge, r, c) ? -9.0f
+                                 : st.sc[(c >> 5) % kScoreRing][lane][c & 31];
                 float v1, v2, mx;
                 int b = 0;
                 v1 = dMI + qMMp + dIMp;
@@ -149,7 +223,7 @@ dp1_kernel(const Dp1Args a)
                 v2 = lND + dDDp;
                 const float nND = hmax(v1, v2);
                 if (mx < nND) { mx = nND; b = 1; }
-                B[(long long)r * ld + c] = (uint8_t)b;
+                st.bt[(c >> 5) % kBtckRing][lane][c & 31] = (uint8_t)b;
                 lMM = nMM; lMI = nMI; lIM = nIM; lDN = nDN; lND = nND;
                 if (lane == 31) {
                     strip[0 * ld + c] = nMM; strip[1 * ld + c] = nMI; strip[2 * ld + c] = nIM;
@@ -159,6 +233,10 @@ dp1_kernel(const Dp1Args a)
             dMM = uMM; dMI = uMI; dIM = uIM; dDN = uDN; dND = uND;
             __syncwarp();
         }
+        // the steps s = 32k+63 < Ld+31 wrote back chunks 0 .. (Ld-1)/32 - 1;
+        // the last chunk is complete after the final step
+        __syncwarp();
+        store_btck_chunk(st, B, ld, r0, Lq, Ld, nchunks - 1, lane);
         __syncwarp();
     }
     // first cell in row-major order among equal maxima
@@ -189,7 +267,6 @@ dp1_finalize_kernel(const Dp1Args a, float thld)
     const int pl = blockIdx.x * kWarpsPerBlock + w;
     if (pl >= a.nprof) return;
     const int p = a.p0 + pl;
-    const int Ld = a.db.plen[p];
     const long long colb = a.db.pstart[p] - a.col0;
     const float* __restrict__ S = a.scores + colb;
     const uint8_t* __restrict__ B = a.btck + colb;
@@ -305,8 +382,8 @@ pass_compact_kernel(const Dp1Args a, int* __restrict__ pass_idx, long long* __re
 void launch_dp1(const Dp1Args& a, cudaStream_t stream)
 {
     if (a.nprof <= 0) return;
-    const int blocks = (int)ceil_div(a.nprof, kWarpsPerBlock);
-    dp1_kernel<<<blocks, 32 * kWarpsPerBlock, 0, stream>>>(a);
+    const int blocks = (int)ceil_div(a.nprof, kDpWarps);
+    dp1_kernel<<<blocks, 32 * kDpWarps, 0, stream>>>(a);
     CBP_CHECK_LAUNCH();
 }
 
