@@ -230,7 +230,9 @@ def main():
     import cother_b200 as cb
     from cother_b200 import synth
     ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
-    q, db = synth.make_workload(args.workload, seed=args.seed + 1000 * rank, ndb=args.ndb)
+    # one query for all ranks; each rank holds its own database shard
+    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=args.ndb,
+                                db_seed=args.seed + 1000 * rank)
     Lq, Ndb = q.npositions, db.npositions
     steps_ddms = total_ddms_steps(q, db)
 
@@ -259,10 +261,16 @@ def main():
     e0.record(stream)
     d2h = 0
     nhits = 0
+    merged_hits = 0
     for _ in range(args.steps):
         bp.process_score_matrix(q)
         recs = bp.hit_records()
         rows = bp.alignment_rows()
+        if dist is not None:
+            # the path's one exchange: the shards' hit lists, merged by E-value
+            from cother_b200 import sharding
+            parts = sharding.gather_hits(sharding.local_hits(bp, rank * db.nprofiles, Lq))
+            merged_hits = len(sharding.merge_hit_lists(parts))
         d2h = recs.nbytes + rows.nbytes
         nhits = len(recs)
         st = bp.stage_times()
@@ -314,6 +322,7 @@ def main():
                         "h2d_bytes_per_step": int(Lq * (4 * 20 + 4 * 3 + 4 * 100 + 2) + 4 * 7 * (Lq + 1)),
                         "d2h_bytes_per_step": int(d2h)},
                 "hits": nhits,
+                "merged_hits": merged_hits if world > 1 else None,
                 "stage_ms": {k: v / steps for k, v in zip(STAGES, stage_acc)},
                 "gpu_launches": launches, "roofline": roof, "clocks": clocks}
         if not args.no_cpu_baseline:

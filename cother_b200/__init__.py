@@ -83,6 +83,7 @@ def load_library(path: str | None = None):
         "cbp_get_hit_records": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_get_search_space": (i32, [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(sz)]),
         "cbp_get_alignments": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
+        "cbp_get_hit_list": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_dp1_noalloc": (i32, [vp, sz, i32, vp, ctypes.c_longlong, i32, vp, vp, vp, i32, i32,
                                   ctypes.c_longlong, vp, vp, vp, vp]),
         "cbp_set_karlin_altschul": (i32, [vp, f32, f32, f32, f32, f32, f32]),
@@ -272,6 +273,18 @@ class BatchProcessing:
             Ld = int(self._db.lens[p])
             term = int(recs["pro_new_dst"][k]) + k * query_len + Ld + query_len - 1
             out.append(tuple(bytes(rows[r, term - n:term]).decode() for r in range(5)))
+        return out
+
+    def hit_list(self) -> np.ndarray:
+        """Record indices of the reported hits of the last search (log E at
+        most the threshold, realigned), sorted by log E-value: the order of
+        the reference's finalizer."""
+        L = load_library()
+        n = ctypes.c_size_t()
+        _check(L.cbp_get_hit_list(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, np.int32)
+        if n.value:
+            _check(L.cbp_get_hit_list(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
         return out
 
     def search_space(self):

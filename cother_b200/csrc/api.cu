@@ -802,6 +802,30 @@ int cbp_get_hit_records(cbp_context* c, float* recs, size_t max_records, size_t*
     });
 }
 
+int cbp_get_hit_list(cbp_context* c, int32_t* order, size_t max_hits, size_t* nhits)
+{
+    return guarded([&] {
+        check_ctx(c);
+        const size_t n = c->h_recs.size() / kRecFloats;
+        std::vector<int32_t> idx;
+        for (size_t i = 0; i < n; i++) {
+            const float* r = c->h_recs.data() + i * kRecFloats;
+            int32_t alnlen;
+            std::memcpy(&alnlen, &r[rEpA], 4);
+            if (r[rEvalue] <= c->logE_thld && alnlen >= 1) idx.push_back((int32_t)i);
+        }
+        std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) {
+            return c->h_recs[(size_t)a * kRecFloats + rEvalue] <
+                   c->h_recs[(size_t)b * kRecFloats + rEvalue];
+        });
+        if (nhits) *nhits = idx.size();
+        if (order) {
+            if (max_hits < idx.size()) throw Error(CBP_ERR_ARG, "hit buffer too small");
+            std::memcpy(order, idx.data(), idx.size() * sizeof(int32_t));
+        }
+    });
+}
+
 int cbp_get_alignments(cbp_context* c, char* rows, size_t row_stride, size_t* length)
 {
     return guarded([&] {

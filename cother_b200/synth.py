@@ -167,14 +167,16 @@ HOMOLOG_FRACTION = 0.01
 
 
 def make_workload(name: str, seed: int = 7, ndb: int | None = None, qindex: int = 0,
-                  homologs: float = HOMOLOG_FRACTION):
+                  homologs: float = HOMOLOG_FRACTION, db_seed: int | None = None):
     """(query ProfileSet, database ProfileSet) for a named workload; a
     fraction `homologs` of the database profiles are planted homologs of
-    the query."""
+    the query. The query depends on `seed` only; the database on `db_seed`
+    (default `seed`), so that shards of one search can share the query."""
     w = WORKLOADS[name]
-    lens = db_lengths(name, seed, ndb)
-    db = make_profiles(lens, seed=seed * 1000 + 1, predicted=False, window=w["window"])
+    dseed = seed if db_seed is None else db_seed
+    lens = db_lengths(name, dseed, ndb)
+    db = make_profiles(lens, seed=dseed * 1000 + 1, predicted=False, window=w["window"])
     q = make_profiles([w["qlens"][qindex]], seed=seed * 1000 + 2 + qindex, predicted=True,
                       window=w["window"])
-    plant_homologs(q, db, homologs, seed=seed * 1000 + 3 + qindex)
+    plant_homologs(q, db, homologs, seed=dseed * 1000 + 3 + qindex)
     return q, db

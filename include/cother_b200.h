@@ -182,6 +182,15 @@ int cbp_get_hit_records(cbp_context* ctx, float* recs, size_t max_records, size_
  * NULL only *length is returned. */
 int cbp_get_alignments(cbp_context* ctx, char* rows, size_t row_stride, size_t* length);
 
+/* The hits of the last cbp_process() call that the reference's finalizer
+ * reports, in its order: records whose log E-value is at most the log E
+ * threshold and that were realigned (alignment length >= 1)
+ * (src/libmycu/cupro/CuBatchProcessingFinalizerPlain.cpp:79-92), sorted by
+ * log E-value, smallest first (CuBatchProcessingFinalizer.cpp:283-292; equal
+ * values keep database order). order[i] receives the record index of the
+ * i-th hit; with order == NULL only the count is returned. */
+int cbp_get_hit_list(cbp_context* ctx, int32_t* order, size_t max_hits, size_t* nhits);
+
 /* Effective search space and length adjustment of the last cbp_process()
  * call (AbstractScoreMatrix::ComputeLengthAdjustment,
  * src/libpro/srcsco/AbstractScoreMatrix.cpp:247-393). */

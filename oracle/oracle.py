@@ -331,3 +331,36 @@ def map_pair(query, db, p, S, M, epa, minpp=0.28, modscores=True, printsss=True)
     return {"fb": fb, "btck": bt, "aln": [b.value.decode() for b in bufs], "alnlen": mo.alnlen,
             "idts": mo.idts, "psts": mo.psts, "gaps": mo.gaps, "beg": mo.beg, "end": mo.end,
             "logz": mo.logz, "maxlogprob": mo.maxlogprob, "mapmax": mo.mapmax}
+
+
+# ---------------------------------------------------------------------------
+# the whole search path
+def search(query, db, ss_table, db_len, n_seqs, ssswgt=0.12, ddmswgt=0.2, dstsegm=6, minpp=0.28,
+           ssemodel=2, xuninf=1, nthreads=1, first_profile=0):
+    """The oracle's search of `query` against `db`: score matrix, phase 1,
+    statistics with E-values for a database of `db_len` positions and
+    `n_seqs` profiles, MAP realignment, and the hits the reference's
+    finalizer reports (log E at most the threshold, realigned), sorted by
+    log E-value with ties in database order. Returns
+    [(profile + first_profile, log E, (5 alignment rows))]."""
+    Lq = query.npositions
+    sc, ms = score_matrix(query, db, ss_table, ssswgt=ssswgt, ddmswgt=ddmswgt, dstsegm=dstsegm,
+                          nthreads=nthreads)
+    thld, lthld = score_threshold(Lq, db_len)
+    sspace, _ = length_adjustment(Lq, db_len, n_seqs)
+    rec, _ = dp1(query, db, sc, 0, 0, db.nprofiles, thld)
+    hits = []
+    for p in np.nonzero(rec["passed"])[0]:
+        s0, Ld = int(db.starts[p]), int(db.lens[p])
+        st, _ = pair_statistics(sc[:, s0:s0 + Ld], query.aa, db.aa[s0:s0 + Ld], rec["score"][p],
+                                rec["psts"][p], Lq, Ld, query.eno[0], db.eno[p], sspace,
+                                ssemodel=ssemodel, xuninf=xuninf)
+        logE = float(np.float32(st[2]))
+        if logE > lthld:
+            continue
+        m = map_pair(query, db, p, sc[:, s0:s0 + Ld], ms[:, s0:s0 + Ld], st[3], minpp=minpp,
+                     modscores=ssswgt > 0, printsss=ssswgt > 0)
+        if m["alnlen"] >= 1:
+            hits.append((int(p) + first_profile, logE, tuple(m["aln"])))
+    hits.sort(key=lambda h: h[1])   # stable: ties keep database order
+    return hits
