@@ -84,6 +84,8 @@ def load_library(path: str | None = None):
         "cbp_get_search_space": (i32, [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(sz)]),
         "cbp_get_alignments": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_get_hit_list": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
+        "cbp_share_database": (i32, [vp, vp]),
+        "cbp_device_memory": (i32, [i32, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
         "cbp_dp1_noalloc": (i32, [vp, sz, i32, vp, ctypes.c_longlong, i32, vp, vp, vp, i32, i32,
                                   ctypes.c_longlong, vp, vp, vp, vp]),
         "cbp_set_karlin_altschul": (i32, [vp, f32, f32, f32, f32, f32, f32]),
@@ -120,6 +122,13 @@ REC_FIELDS = ["score", "org_pro_no", "pro_new_dst", "psts", "beg_coords", "end_c
               "lambda_est", "K_est", "log_evalue", "log_evalue_pair", "min", "max", "expected",
               "entropy", "lambda", "K", "identities", "gaps"]
 _REC_UINT = {"org_pro_no", "pro_new_dst", "beg_coords", "end_coords"}
+
+
+def device_memory(device: int = 0):
+    """(free, total) device memory in bytes."""
+    f, t = ctypes.c_size_t(), ctypes.c_size_t()
+    _check(load_library().cbp_device_memory(int(device), ctypes.byref(f), ctypes.byref(t)))
+    return int(f.value), int(t.value)
 
 
 def records_table(recs: np.ndarray) -> dict:
@@ -196,6 +205,11 @@ class BatchProcessing:
         beg, end = db.field_tables()
         _check(load_library().cbp_transfer_chunk(self._h, beg, end, None))
         self._db = db
+
+    def share_database(self, owner: "BatchProcessing") -> None:
+        """Search `owner`'s resident database (same device) without a copy."""
+        _check(load_library().cbp_share_database(self._h, owner._h))
+        self._db = owner._db
 
     def process_score_matrix(self, query, query_serial: int = 0) -> None:
         """Search one query profile against the resident chunk."""

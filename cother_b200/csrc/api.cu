@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -128,6 +129,10 @@ struct ProfilesStore {
     ProfilesDev view;
     std::vector<int> h_plen;
     std::vector<long long> h_pstart;
+    ProfilesStore() = default;
+    ProfilesStore(const ProfilesStore&) = delete;
+    ProfilesStore& operator=(const ProfilesStore&) = delete;
+    ~ProfilesStore() { release(); }
     void release() {
         for (DevBuf* b : {&tf, &ss, &dst, &dstlen, &trn, &bkg, &eno, &plen, &pstart, &pro, &aa, &sss})
             b->release();
@@ -148,7 +153,10 @@ struct cbp_context {
     float sstab_h[kSSCard * kSSCard];
     float dmstab_h[kDstCard * kDstCard];
     DevBuf sstab, dmstab;
-    ProfilesStore db, query;
+    // the resident database chunk; contexts on one device may share it
+    // (cbp_share_database), the last owner frees it
+    std::shared_ptr<ProfilesStore> db = std::make_shared<ProfilesStore>();
+    ProfilesStore query;
     bool have_db = false;
     size_t mem_budget = 0;
     size_t max_slab_positions = 0;
@@ -343,7 +351,7 @@ struct Slab { int p0, p1; long long col0; int ncols; };
 
 std::vector<Slab> plan_slabs(const cbp_context* c, int Lq)
 {
-    const ProfilesStore& db = c->db;
+    const ProfilesStore& db = *c->db;
     const int P = (int)db.h_plen.size();
     // bytes per slab position: scores + modscores + backtrack byte per query
     // position, the DP band strip and per-profile records
@@ -447,7 +455,7 @@ int cbp_destroy(cbp_context* c)
     if (!c) return CBP_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    c->db.release();
+    c->db.reset();
     c->query.release();
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax, &c->dpcoords,
                       &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
@@ -492,7 +500,36 @@ int cbp_transfer_chunk(cbp_context* c, char* const* beg, char* const* end, const
     return guarded([&] {
         check_ctx(c);
         c->have_db = false;
-        upload_profiles(c->db, beg, end, c->stream);
+        // a fresh store: contexts sharing the previous one keep it
+        auto st = std::make_shared<ProfilesStore>();
+        upload_profiles(*st, beg, end, c->stream);
+        c->db = std::move(st);
+        c->have_db = true;
+    });
+}
+
+int cbp_device_memory(int device, size_t* free_bytes, size_t* total_bytes)
+{
+    return guarded([&] {
+        if (!free_bytes || !total_bytes) throw Error(CBP_ERR_ARG, "null output pointer");
+        int ndev = 0;
+        CBP_CUDA(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev) throw Error(CBP_ERR_ARG, "invalid device");
+        CBP_CUDA(cudaSetDevice(device));
+        CBP_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
+    });
+}
+
+int cbp_share_database(cbp_context* c, cbp_context* owner)
+{
+    return guarded([&] {
+        check_ctx(c);
+        check_ctx(owner);
+        if (c->device != owner->device)
+            throw Error(CBP_ERR_ARG, "contexts on different devices cannot share a database");
+        if (!owner->have_db) throw Error(CBP_ERR_STATE, "the owner has no database chunk");
+        CBP_CUDA(cudaStreamSynchronize(owner->stream));   // its upload has completed
+        c->db = owner->db;
         c->have_db = true;
     });
 }
@@ -521,8 +558,8 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             // the query length and the database totals default to this
             // query and this chunk when not set
             const size_t m = c->query_len ? c->query_len : (size_t)Lq;
-            const unsigned long long n = c->db_len ? c->db_len : (unsigned long long)c->db.view.N;
-            const size_t N = c->n_seqs ? c->n_seqs : (size_t)c->db.view.P;
+            const unsigned long long n = c->db_len ? c->db_len : (unsigned long long)c->db->view.N;
+            const size_t N = c->n_seqs ? c->n_seqs : (size_t)c->db->view.P;
             length_adjustment(c->gap_lambda, c->gap_K, c->gap_alpha, c->gap_beta, m, n, N,
                               &c->searchspace, &c->delta_length);
             // thresholds not set by the caller follow from EVAL as the
@@ -553,7 +590,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         for (const Slab& s : slabs) {
             ScoreArgs a;
             a.q = c->query.view;
-            a.db = c->db.view;
+            a.db = c->db->view;
             a.col0 = s.col0;
             a.ncols = s.ncols;
             a.ld = align_up(s.ncols, 32);
@@ -572,7 +609,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             d.ld = a.ld;
             d.Lq = Lq;
             d.qtrn = c->query.view.trn;
-            d.db = c->db.view;
+            d.db = c->db->view;
             d.col0 = s.col0;
             d.p0 = s.p0;
             d.nprof = s.p1 - s.p0;
@@ -622,7 +659,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 st.Lq = Lq;
                 st.col0 = s.col0;
                 st.p0 = s.p0;
-                st.db = c->db.view;
+                st.db = c->db->view;
                 st.qaa = c->query.view.aa;
                 st.qeno = c->query_eno;
                 st.x_uninf = c->opt.x_uninf;
@@ -663,7 +700,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                     mp.Lq = Lq;
                     mp.col0 = s.col0;
                     mp.p0 = s.p0;
-                    mp.db = c->db.view;
+                    mp.db = c->db->view;
                     mp.qtrn = c->query.view.trn;
                     mp.qaa = c->query.view.aa;
                     mp.qsss = c->query.view.sss;

@@ -105,6 +105,20 @@ int cbp_set_logE_threshold(cbp_context* ctx, float log_threshold);
 int cbp_transfer_chunk(cbp_context* ctx, char* const* pmbeg, char* const* pmend,
                        const size_t* szfields);
 
+/* Use `owner`'s resident database chunk instead of a copy of one's own (no
+ * counterpart in the reference, where each worker transfers its chunk).
+ * Several contexts on one device can then search the same resident database
+ * at the same time, each on its own stream with its own working memory,
+ * which is what a request loop that keeps several queries in flight needs.
+ * The chunk lives until its last user transfers another chunk or is
+ * destroyed. Both contexts must be on the same device. */
+int cbp_share_database(cbp_context* ctx, cbp_context* owner);
+
+/* Free and total device memory of `device` in bytes (cudaMemGetInfo), for
+ * callers that divide it between contexts (no counterpart in the
+ * reference, whose CuDeviceMemory does the same internally). */
+int cbp_device_memory(int device, size_t* free_bytes, size_t* total_bytes);
+
 /* Search one query against the resident chunk
  * (CuBatchProcessing::ProcessScoreMatrix, :87-99). `qpmbeg`/`qpmend` are
  * the pointer tables of the query's field arrays (one profile). The call
