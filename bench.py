@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", action="store_true",
+                    help="request loop over a resident database: queries/s and p50/p99 latency")
+    ap.add_argument("--rate", type=float, default=5.0, help="--serve: offered load (Poisson, queries/s)")
+    ap.add_argument("--queries", type=int, default=12, help="--serve: requests in the timed run")
+    ap.add_argument("--slots", type=int, default=3, help="--serve: concurrent requests")
     return ap.parse_args()
 
 
@@ -211,10 +216,51 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_serve(args):
+    """--serve: Poisson arrivals of request queries against a resident
+    database, served by concurrent slots (cother_b200.serving); reports the
+    completed queries per second and the latency (arrival to results)."""
+    import cother_b200 as cb
+    from cother_b200 import synth
+    from cother_b200.serving import SearchServer, latency_summary
+    workload = args.workload if args.workload != DEFAULT_WORKLOAD else "serve_db100k"
+    ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
+    _, db = synth.make_workload(workload, seed=args.seed, ndb=args.ndb)
+    queries = synth.serving_queries(args.queries + 1, seed=args.seed)
+    rng = np.random.default_rng(args.seed)
+    gaps = rng.exponential(1.0 / args.rate, args.queries)
+    with SearchServer(db, ss, slots=args.slots) as srv:
+        srv.submit(queries[-1]).result()           # warm-up, not timed
+        t0 = time.perf_counter()
+        futs = []
+        for k in range(args.queries):
+            t0 += gaps[k]
+            delay = t0 - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futs.append(srv.submit(queries[k]))
+        res = [f.result() for f in futs]
+        budget = srv.ledger.budget
+    s = latency_summary(res)
+    cells = sum(q.npositions for q in queries[:args.queries]) * db.npositions
+    wall = max(r["finish"] for r in res) - min(r["arrival"] for r in res)
+    print(json.dumps({
+        "metric": "queries_per_s", "value": s["queries_per_s"], "unit": "queries/s",
+        "n_gpus": 1, "higher_is_better": True, "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"],
+        "service_p50_ms": s["service_p50_ms"], "offered_qps": args.rate, "queries": args.queries,
+        "gcups": cells / wall / 1e9, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload, "db_profiles": db.nprofiles, "db_positions": db.npositions,
+                   "query_lens": [q.npositions for q in queries[:args.queries]],
+                   "slots": args.slots, "memory_budget_bytes": budget}}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.serve:
+        run_serve(args)
         return
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))

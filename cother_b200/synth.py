@@ -151,7 +151,18 @@ WORKLOADS = {
     "qsweep_db50k": dict(qlens=[64, 256, 1024], ndb=50000, law=("lognormal", 220, 30, 1500), window=64),
     # 1 query of length 1,500 vs 20,000 profiles of length U(500,1500), window 128
     "q1500_db20k": dict(qlens=[1500], ndb=20000, law=("uniform", 500, 1500), window=128),
+    # serving: a resident 100,000-profile database (lognormal median 220 in
+    # [30,1500]); request queries have lognormal lengths, median 250 in
+    # [40,1200] (serving_queries)
+    "serve_db100k": dict(qlens=[250], ndb=100000, law=("lognormal", 220, 30, 1500), window=64),
 }
+
+
+def serving_queries(n: int, seed: int = 7):
+    """`n` request queries with lognormal lengths (median 250, in [40,1200])."""
+    lens = lognormal_lengths(n, 250, 40, 1200, seed=seed * 1000 + 11)
+    return [make_profiles([int(L)], seed=seed * 1000 + 100 + k, predicted=True)
+            for k, L in enumerate(lens)]
 
 
 def db_lengths(name: str, seed: int = 7, ndb: int | None = None) -> np.ndarray:
