@@ -19,6 +19,7 @@ collective on the data path; the time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import subprocess
@@ -53,6 +54,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tc", default="plain", choices=["plain", "bf16", "tf32"],
+                    help="form of the profile-profile term: FP32 CUDA cores or tensor cores "
+                         "(BF16x3 / TF32x3 hi-lo split)")
     ap.add_argument("--serve", action="store_true",
                     help="request loop over a resident database: queries/s and p50/p99 latency")
     ap.add_argument("--rate", type=float, default=5.0, help="--serve: offered load (Poisson, queries/s)")
@@ -282,7 +286,9 @@ def main():
     Lq, Ndb = q.npositions, db.npositions
     steps_ddms = total_ddms_steps(q, db)
 
-    bp = cb.BatchProcessing(ss, device=local)
+    opts = cb.Options.defaults()
+    opts.tc_form = {"plain": cb.TC_PLAIN, "bf16": cb.TC_BF16X3, "tf32": cb.TC_TF32X3}[args.tc]
+    bp = cb.BatchProcessing(ss, opts, device=local)
     bp.transfer_cpm_data(db)
     db_len, nseqs = Ndb * world, db.nprofiles * world
     bp.set_db_details(db_len, nseqs)
@@ -319,6 +325,7 @@ def main():
             merged_hits = len(sharding.merge_hit_lists(parts))
         d2h = recs.nbytes + rows.nbytes
         nhits = len(recs)
+        order = bp.hit_list()
         st = bp.stage_times()
         stage_acc = [a + b for a, b in zip(stage_acc, st)]
         kern_ms += sum(st)
@@ -361,13 +368,15 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
                 "config": {"workload": args.workload, "query_len": Lq, "db_profiles": db.nprofiles,
-                           "db_positions": Ndb, "stages": STAGES,
+                           "db_positions": Ndb, "stages": STAGES, "tc_form": args.tc,
                            "l2": "inputs larger than L2 (database chunk > 126 MB)",
                            "parallelism": f"dp{world} (database shard per GPU)"},
                 "e2e": {"value": e2e, "unit": "GCUPS",
                         "h2d_bytes_per_step": int(Lq * (4 * 20 + 4 * 3 + 4 * 100 + 2) + 4 * 7 * (Lq + 1)),
                         "d2h_bytes_per_step": int(d2h)},
                 "hits": nhits,
+                "top50_digest": hashlib.sha1(
+                    recs[order[:50], 1].view(np.uint32).tobytes()).hexdigest()[:16],
                 "merged_hits": merged_hits if world > 1 else None,
                 "stage_ms": {k: v / steps for k, v in zip(STAGES, stage_acc)},
                 "gpu_launches": launches, "roofline": roof, "clocks": clocks}

@@ -34,6 +34,9 @@ class CbpError(RuntimeError):
         self.code = code
 
 
+TC_PLAIN, TC_BF16X3, TC_TF32X3 = 0, 1, 2   # Options.tc_form
+
+
 class Options(ctypes.Structure):
     """Path options (``cbp_options``; MOptions of the reference)."""
 
@@ -41,7 +44,7 @@ class Options(ctypes.Structure):
         ("ssswgt", ctypes.c_float), ("cvswgt", ctypes.c_float), ("ddmswgt", ctypes.c_float),
         ("dstsegm", ctypes.c_int), ("mapaln", ctypes.c_int), ("minpp", ctypes.c_float),
         ("ssemodel", ctypes.c_int), ("x_uninf", ctypes.c_int), ("eval", ctypes.c_float),
-        ("nohits", ctypes.c_int), ("noalns", ctypes.c_int),
+        ("nohits", ctypes.c_int), ("noalns", ctypes.c_int), ("tc_form", ctypes.c_int),
     ]
 
     @classmethod

@@ -33,6 +33,7 @@ CUDA_SOURCES = [
     "stats_kernel.cu",
     "map_kernel.cu",
     "dp1_noalloc.cu",
+    "tc_kernel.cu",
 ]
 CUDA_HEADERS = [
     "map_kernel.cuh",
@@ -42,6 +43,7 @@ CUDA_HEADERS = [
     "layout.h",
     "score_kernel.cuh",
     "dp1_kernel.cuh",
+    "tc_kernel.cuh",
 ]
 
 
@@ -78,7 +80,7 @@ def build_main(force: bool = False, verbose_ptxas: bool = False) -> str:
     if not force and _newer(LIB_MAIN, deps):
         return LIB_MAIN
     tmp = LIB_MAIN + ".tmp"
-    cmd = [_nvcc(), "-shared", "-o", tmp] + nvcc_flags(verbose_ptxas) + srcs + ["-lpthread"]
+    cmd = [_nvcc(), "-shared", "-o", tmp] + nvcc_flags(verbose_ptxas) + srcs + ["-lcublas", "-lpthread"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB_MAIN)
     return LIB_MAIN

@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "layout.h"
 #include "score_kernel.cuh"
+#include "tc_kernel.cuh"
 #include "dp1_kernel.cuh"
 #include "stats_kernel.cuh"
 #include "map_kernel.cuh"
@@ -153,6 +154,9 @@ struct cbp_context {
     float sstab_h[kSSCard * kSSCard];
     float dmstab_h[kDstCard * kDstCard];
     DevBuf sstab, dmstab;
+    // tensor-core form of the profile-profile term
+    cublasHandle_t cublas = nullptr;
+    DevBuf tcq_hi, tcq_lo, tcd_hi, tcd_lo;
     // the resident database chunk; contexts on one device may share it
     // (cbp_share_database), the last owner frees it
     std::shared_ptr<ProfilesStore> db = std::make_shared<ProfilesStore>();
@@ -358,7 +362,8 @@ std::vector<Slab> plan_slabs(const cbp_context* c, int Lq)
     // scores 4 + modscores 4 + phase-1 backtrack 1, and the phase-2 buffers
     // for the worst case of every profile realigned: forward-backward 4 +
     // MAP backtrack 1 + alignment rows 5; strips and records per position
-    const size_t per_pos = (size_t)Lq * 19 + 10 * 4 + 128;
+    size_t per_pos = (size_t)Lq * 19 + 10 * 4 + 128;
+    if (c->opt.tc_form != CBP_TC_PLAIN) per_pos += 2 * tc_operand_bytes(c->opt.tc_form, 1);
     size_t cap = c->mem_budget / per_pos;
     if (c->max_slab_positions) cap = std::min(cap, c->max_slab_positions);
     cap = std::min<size_t>(cap, (size_t)1 << 30);
@@ -398,6 +403,7 @@ void cbp_default_options(cbp_options* o)
     o->eval = 10.0f;
     o->nohits = 700;
     o->noalns = 700;
+    o->tc_form = CBP_TC_PLAIN;
 }
 
 const char* cbp_last_error(void) { return g_last_error.c_str(); }
@@ -420,6 +426,8 @@ int cbp_create(int device, const cbp_options* opt, const float* ss_table, size_t
         if (opt->ssemodel < 0 || opt->ssemodel > 2) throw Error(CBP_ERR_ARG, "SSEMODEL must be 0, 1 or 2");
         if (!(opt->minpp >= 0.0f && opt->minpp < 1.0f)) throw Error(CBP_ERR_ARG, "MINPP must be in [0,1)");
         if (!(opt->eval >= 0.0f)) throw Error(CBP_ERR_ARG, "EVAL must be >= 0");
+        if (opt->tc_form < CBP_TC_PLAIN || opt->tc_form > CBP_TC_TF32X3)
+            throw Error(CBP_ERR_ARG, "tc_form must be CBP_TC_PLAIN, CBP_TC_BF16X3 or CBP_TC_TF32X3");
         int ndev = 0;
         CBP_CUDA(cudaGetDeviceCount(&ndev));
         if (device < 0 || device >= ndev) throw Error(CBP_ERR_ARG, "invalid device");
@@ -463,6 +471,8 @@ int cbp_destroy(cbp_context* c)
         b->release();
     c->sstab.release();
     c->dmstab.release();
+    for (DevBuf* b : {&c->tcq_hi, &c->tcq_lo, &c->tcd_hi, &c->tcd_lo}) b->release();
+    if (c->cublas) cublasDestroy(c->cublas);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -603,6 +613,27 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             a.dmstab = c->dmstab.as<float>();
             a.scores = c->scores.as<float>();
             a.modscores = c->modscores.as<float>();
+            if (c->opt.tc_form != CBP_TC_PLAIN) {
+                if (!c->cublas) {
+                    if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS)
+                        throw Error(CBP_ERR_CUDA, "cuBLAS handle creation failed");
+                }
+                const int f = c->opt.tc_form;
+                c->tcq_hi.reserve(tc_operand_bytes(f, Lq));
+                c->tcq_lo.reserve(tc_operand_bytes(f, Lq));
+                c->tcd_hi.reserve(tc_operand_bytes(f, s.ncols));
+                c->tcd_lo.reserve(tc_operand_bytes(f, s.ncols));
+                TcArgs t;
+                t.q = a.q;
+                t.db = a.db;
+                t.col0 = a.col0;
+                t.ncols = a.ncols;
+                t.ld = a.ld;
+                t.Lq = Lq;
+                tc_profile_sums(t, f, c->cublas, c->tcq_hi.p, c->tcq_lo.p, c->tcd_hi.p, c->tcd_lo.p,
+                                a.scores, c->stream);
+                a.dots_in_scores = true;
+            }
 
             Dp1Args d;
             d.scores = a.scores;

@@ -271,11 +271,15 @@ score_matrix_kernel(const ScoreArgs a)
 
         // profile-profile term (CuBatchScoreMatrix_Init.cu:159-186)
         float acc = 0.0f;
+        if (a.dots_in_scores) {
+            acc = a.scores[(long long)row * a.ld + col];
+        } else {
 #pragma unroll
-        for (int k = 0; k < kNAA; k++) {
-            const float num = s_qtf[r][k] * s_dtf[k][lane];
-            const float den = 0.5f * (s_qbg[k] + s_dbg[k][lane]);
-            acc = acc + __fdiv_rn(num, den);
+            for (int k = 0; k < kNAA; k++) {
+                const float num = s_qtf[r][k] * s_dtf[k][lane];
+                const float den = 0.5f * (s_qbg[k] + s_dbg[k][lane]);
+                acc = acc + __fdiv_rn(num, den);
+            }
         }
         float s = cb_logf(acc) - a.initshift;
         float mod = 0.0f;

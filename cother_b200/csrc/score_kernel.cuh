@@ -19,6 +19,9 @@ struct ScoreArgs {
     const float* dmstab = nullptr;  // [22][22]
     float* scores = nullptr;        // [Lq][ld]
     float* modscores = nullptr;     // [Lq][ld]
+    // tensor-core form: the profile-profile sums, computed beforehand into
+    // `scores` ([Lq][ld]), which the kernel then overwrites with the scores
+    bool dots_in_scores = false;
 };
 
 void launch_score_matrix(const ScoreArgs& a, cudaStream_t stream);

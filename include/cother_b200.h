@@ -50,8 +50,13 @@ enum {
 typedef struct cbp_context cbp_context;
 
 /* Options of the path (src/libpro/srcpro/MOptions.cpp:76-147). */
+/* Forms of the profile-profile term (cbp_options.tc_form). */
+#define CBP_TC_PLAIN 0    /* FP32 CUDA cores, the reference's operation order */
+#define CBP_TC_BF16X3 1   /* tensor cores: BF16 hi/lo split, three products, FP32 accumulate */
+#define CBP_TC_TF32X3 2   /* tensor cores: TF32 hi/lo split, three products, FP32 accumulate */
+
 typedef struct cbp_options {
-    float ssswgt;     /* SSSWGT: weight of the SS score (> 0) */
+    float ssswgt;     /* SSSWGT: weight of the SS score, [0,1) */
     float cvswgt;     /* CVSWGT: context-vector term; must be 0 (term off) */
     float ddmswgt;    /* DDMSWGT: weight of the DDMS score */
     int   dstsegm;    /* DSTSEGM: minimum DDMS segment length */
@@ -62,6 +67,14 @@ typedef struct cbp_options {
     float eval;       /* EVAL: E-value threshold */
     int   nohits;     /* NOHITS */
     int   noalns;     /* NOALNS */
+    int   tc_form;    /* CBP_TC_*: how the profile-profile term is computed. The
+                       * tensor-core forms recast it, for each database profile,
+                       * as the contraction [Lq x 20] x [20 x Ld] of the query's
+                       * target frequencies with the profile's frequencies divided
+                       * by the mean background (no counterpart in the reference,
+                       * which sums the 20 quotients on CUDA cores); results agree
+                       * with the plain form within about 1e-6 relative, not bit
+                       * for bit. */
 } cbp_options;
 
 /* Fill *opt with the values of the parity configuration:

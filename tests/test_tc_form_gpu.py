@@ -1,0 +1,78 @@
+"""The tensor-core forms of the profile-profile term (BF16x3 and TF32x3
+through cuBLAS) against the plain FP32 form and an FP64 restatement.
+
+With the SS and DDMS terms off, a cell's score is log(sum) - shift, where
+sum = sum_a q_a d_a / (0.5 (qbg_a + dbg_a)); the test computes the sums in
+FP64 and bounds each form's error (the plain form is the reference's FP32
+operation order). With every term on, the forms must report the same top
+hits in the same order, scores within 1e-4 and log E-values within 1e-3
+relative of the plain form."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _scores(q, db, ss, **opt):
+    import cother_b200 as cb
+    o = cb.Options.defaults()
+    for k, v in opt.items():
+        setattr(o, k, v)
+    with cb.BatchProcessing(ss, o) as bp:
+        bp.set_score_threshold(3.0e38)
+        bp.transfer_cpm_data(db)
+        bp.process_score_matrix(q)
+        sc, _, _ = bp.read_score_matrix(q.npositions, db.npositions)
+    return sc.astype(np.float64)
+
+
+def test_forms_against_fp64(ss_table):
+    import cother_b200 as cb
+    from cother_b200 import synth
+    q = synth.make_profiles([130], 951, True)
+    db = synth.make_profiles(synth.lognormal_lengths(30, 150, 30, 400, seed=952), 953, False)
+    qtf = q.tf.astype(np.float64)                       # [20][Lq]
+    qbg = q.bkg[:, 0].astype(np.float64)
+    dtf = db.tf.astype(np.float64)                      # [20][N]
+    dbg = db.bkg.astype(np.float64)[:, db.addrpro]      # [20][N]
+    w = dtf / (0.5 * (qbg[:, None] + dbg))
+    ref = np.log(qtf.T @ w) - 0.002                     # MAPALN=1 shift
+    errs = {}
+    for name, form in (("plain", cb.TC_PLAIN), ("bf16x3", cb.TC_BF16X3), ("tf32x3", cb.TC_TF32X3)):
+        sc = _scores(q, db, ss_table, ssswgt=0.0, ddmswgt=0.0, tc_form=form)
+        errs[name] = float(np.max(np.abs(sc - ref)))
+    # a few float32 ulps of the log; the split forms keep about FP32 accuracy
+    assert errs["plain"] < 2e-6, errs
+    assert errs["bf16x3"] < 2e-5, errs
+    assert errs["tf32x3"] < 2e-5, errs
+
+
+def test_forms_report_the_same_top_hits(ss_table):
+    import cother_b200 as cb
+    from cother_b200 import synth
+    q = synth.make_profiles([180], 961, True)
+    db = synth.make_profiles(synth.lognormal_lengths(400, 180, 30, 600, seed=962), 963, False)
+    synth.plant_homologs(q, db, 0.05, seed=964)
+    res = {}
+    for form in (cb.TC_PLAIN, cb.TC_BF16X3, cb.TC_TF32X3):
+        o = cb.Options.defaults()
+        o.tc_form = form
+        with cb.BatchProcessing(ss_table, o) as bp:
+            bp.set_db_details(db.npositions, db.nprofiles)
+            bp.transfer_cpm_data(db)
+            bp.process_score_matrix(q)
+            recs = cb.records_table(bp.hit_records())
+            order = bp.hit_list()
+            res[form] = (recs, order)
+    def top(form, n=50):
+        recs, order = res[form]
+        sel = order[:n]
+        return recs["org_pro_no"][sel], recs["score"][sel], recs["log_evalue"][sel]
+
+    p0, s0, e0 = top(cb.TC_PLAIN)
+    assert len(p0) >= 10
+    for form in (cb.TC_BF16X3, cb.TC_TF32X3):
+        p1, s1, e1 = top(form)
+        assert np.array_equal(p1, p0), form
+        assert np.all(np.abs(s1 - s0) <= 1e-4 * np.abs(s0) + 1e-6), form
+        assert np.all(np.abs(e1 - e0) <= 1e-3 * np.abs(e0) + 1e-6), form
