@@ -89,6 +89,7 @@ def load_library(path: str | None = None):
         "cbp_get_hit_list": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_share_database": (i32, [vp, vp]),
         "cbp_device_memory": (i32, [i32, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
+        "cbp_slab_bytes": (i32, [vp, sz, sz, ctypes.POINTER(sz)]),
         "cbp_dp1_noalloc": (i32, [vp, sz, i32, vp, ctypes.c_longlong, i32, vp, vp, vp, i32, i32,
                                   ctypes.c_longlong, vp, vp, vp, vp]),
         "cbp_set_karlin_altschul": (i32, [vp, f32, f32, f32, f32, f32, f32]),
@@ -132,6 +133,16 @@ def device_memory(device: int = 0):
     f, t = ctypes.c_size_t(), ctypes.c_size_t()
     _check(load_library().cbp_device_memory(int(device), ctypes.byref(f), ctypes.byref(t)))
     return int(f.value), int(t.value)
+
+
+def slab_bytes(query_len: int, positions: int, options: "Options | None" = None) -> int:
+    """Working device memory of one slab of `positions` database positions
+    for a query of `query_len` positions (what the slab planner charges)."""
+    o = options if options is not None else Options.defaults()
+    n = ctypes.c_size_t()
+    _check(load_library().cbp_slab_bytes(ctypes.byref(o), int(query_len), int(positions),
+                                         ctypes.byref(n)))
+    return int(n.value)
 
 
 def records_table(recs: np.ndarray) -> dict:

@@ -176,10 +176,11 @@ struct cbp_context {
     DevBuf nnweights;
     // working buffers
     DevBuf scores, modscores, btck, bandbuf, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
-    DevBuf hitrecs, fb2, strip2, btck2, alnbuf;
+    DevBuf hitrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf;
     std::vector<char> h_alns[5];
     long long base_len = 0, base_npass = 0;   // running phase-2 offsets over slabs
-    long long last_ld2 = 0, last_npos2 = 0;
+    long long last_npos2 = 0;
+    int h_maperr = 0;   // set by the MAP stage when a wait between warps gave up
     bool score_thld_set = false, logE_thld_set = false;
     // results of the last process() call, all slabs
     std::vector<float> h_recs;
@@ -350,6 +351,30 @@ void check_ctx(cbp_context* c)
     CBP_CUDA(cudaSetDevice(c->device));
 }
 
+// Working bytes per slab position for a query of length Lq: score matrix,
+// modular scores and phase-1 backtrack per query row (9 Lq), the phase-1
+// band strip and per-profile records (168), and the phase-2 buffers for the
+// worst case of every profile realigned: cell scores and forward-backward
+// values per row of the padded bands (8 x 32 nb), backtrack and sign words
+// per band (12 nb), band edges (4 x 48) and alignment rows (5, plus the 5 Lq
+// bytes of each pair's slot, counted per position). The tensor-core form
+// adds its operands.
+size_t slab_bytes_per_position(const cbp_options& o, int Lq)
+{
+    const size_t nb = (size_t)map_bands(Lq);
+    size_t b = (size_t)Lq * 9 + 168 + nb * (8 * 32 + 12) + 4 * kMapMaxWarps * kMapEdgeFields + 5 +
+               (size_t)Lq * 5;
+    if (o.tc_form != CBP_TC_PLAIN) b += 2 * tc_operand_bytes(o.tc_form, 1);
+    return b;
+}
+
+// bytes per slab independent of its size: the 31 extra diagonal rows of
+// the phase-2 bands
+size_t slab_fixed_bytes(int Lq)
+{
+    return 31 * (size_t)map_bands(Lq) * (8 * 32 + 12);
+}
+
 // Slabs of whole profiles whose score matrices fit the working budget.
 struct Slab { int p0, p1; long long col0; int ncols; };
 
@@ -357,14 +382,9 @@ std::vector<Slab> plan_slabs(const cbp_context* c, int Lq)
 {
     const ProfilesStore& db = *c->db;
     const int P = (int)db.h_plen.size();
-    // bytes per slab position: scores + modscores + backtrack byte per query
-    // position, the DP band strip and per-profile records
-    // scores 4 + modscores 4 + phase-1 backtrack 1, and the phase-2 buffers
-    // for the worst case of every profile realigned: forward-backward 4 +
-    // MAP backtrack 1 + alignment rows 5; strips and records per position
-    size_t per_pos = (size_t)Lq * 19 + 10 * 4 + 128;
-    if (c->opt.tc_form != CBP_TC_PLAIN) per_pos += 2 * tc_operand_bytes(c->opt.tc_form, 1);
-    size_t cap = c->mem_budget / per_pos;
+    const size_t per_pos = slab_bytes_per_position(c->opt, Lq);
+    const size_t fixed = slab_fixed_bytes(Lq);
+    size_t cap = c->mem_budget > fixed ? (c->mem_budget - fixed) / per_pos : 0;
     if (c->max_slab_positions) cap = std::min(cap, c->max_slab_positions);
     cap = std::min<size_t>(cap, (size_t)1 << 30);
     std::vector<Slab> out;
@@ -467,7 +487,7 @@ int cbp_destroy(cbp_context* c)
     c->query.release();
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax, &c->dpcoords,
                       &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
-                      &c->fb2, &c->strip2, &c->btck2, &c->alnbuf})
+                      &c->cs2, &c->fb2, &c->sg2, &c->bt2, &c->strip2, &c->maperr, &c->alnbuf})
         b->release();
     c->sstab.release();
     c->dmstab.release();
@@ -530,6 +550,16 @@ int cbp_device_memory(int device, size_t* free_bytes, size_t* total_bytes)
     });
 }
 
+int cbp_slab_bytes(const cbp_options* opt, size_t query_len, size_t positions, size_t* bytes)
+{
+    return guarded([&] {
+        if (!opt || !bytes) throw Error(CBP_ERR_ARG, "null options or output pointer");
+        if (query_len < 1 || query_len > (size_t)INT32_MAX) throw Error(CBP_ERR_ARG, "invalid query length");
+        const int Lq = (int)query_len;
+        *bytes = slab_fixed_bytes(Lq) + slab_bytes_per_position(*opt, Lq) * positions;
+    });
+}
+
 int cbp_share_database(cbp_context* c, cbp_context* owner)
 {
     return guarded([&] {
@@ -561,7 +591,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         for (auto& r : c->h_alns) r.clear();
         c->base_len = 0;
         c->base_npass = 0;
-        c->last_ld2 = c->last_npos2 = 0;
+        c->last_npos2 = 0;
         c->query_eno = *reinterpret_cast<const float*>(qbeg[fENO]);
         {
             // effective search space (AbstractScoreMatrix::ComputeLengthAdjustment);
@@ -717,12 +747,16 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 CBP_CUDA(cudaMemcpyAsync(&npos2, c->passcnt.as<char>() + 8, sizeof(long long),
                                          cudaMemcpyDeviceToHost, c->stream));
                 CBP_CUDA(cudaStreamSynchronize(c->stream));
-                const long long ld2 = align_up(npos2, 32);
+                const long long nd = map_diag_rows(npos2);
+                const size_t nb = (size_t)map_bands(Lq);
                 const long long alnstride = align_up(npos2 + (long long)npass * Lq, 32);
                 if (c->opt.mapaln) {
-                    c->fb2.reserve((size_t)Lq * ld2 * sizeof(float));
-                    c->strip2.reserve(5 * (size_t)ld2 * sizeof(float));
-                    c->btck2.reserve((size_t)Lq * ld2);
+                    c->cs2.reserve(nb * nd * 32 * sizeof(float));
+                    c->fb2.reserve(nb * nd * 32 * sizeof(float));
+                    c->sg2.reserve(nb * nd * sizeof(unsigned));
+                    c->bt2.reserve(nb * nd * sizeof(unsigned long long));
+                    c->strip2.reserve((size_t)map_strip_floats(npos2) * sizeof(float));
+                    c->maperr.reserve(sizeof(int));
                     c->alnbuf.reserve(5 * (size_t)alnstride);
                     MapArgs mp;
                     mp.scores = a.scores;
@@ -743,19 +777,24 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                     mp.pass_idx = c->passidx.as<int>();
                     mp.pass_dst = c->passdst.as<long long>();
                     mp.recs = c->hitrecs.as<float>();
+                    mp.nd = nd;
+                    mp.cs = c->cs2.as<float>();
                     mp.fb = c->fb2.as<float>();
+                    mp.sg = c->sg2.as<unsigned>();
+                    mp.bt = c->bt2.as<unsigned long long>();
                     mp.strip = c->strip2.as<float>();
-                    mp.btck = c->btck2.as<uint8_t>();
-                    mp.ld2 = ld2;
+                    mp.err = c->maperr.as<int>();
                     mp.alns = c->alnbuf.as<char>();
                     mp.alnstride = alnstride;
                     CBP_CUDA(cudaMemsetAsync(c->alnbuf.p, 0, 5 * (size_t)alnstride, c->stream));
+                    CBP_CUDA(cudaMemsetAsync(c->maperr.p, 0, sizeof(int), c->stream));
                     CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
                     launch_map(mp, c->stream);
                     CBP_CUDA(cudaEventRecord(c->ev[7], c->stream));
-                    c->launches += 1;
-                    c->stage_launches[4] += 1;
-                    c->last_ld2 = ld2;
+                    CBP_CUDA(cudaMemcpyAsync(&c->h_maperr, c->maperr.p, sizeof(int),
+                                             cudaMemcpyDeviceToHost, c->stream));
+                    c->launches += 2;
+                    c->stage_launches[4] += 2;
                     c->last_npos2 = npos2;
                 }
                 const size_t off = c->h_recs.size();
@@ -775,6 +814,9 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                                                  (size_t)slablen, cudaMemcpyDeviceToHost, c->stream));
                 }
                 CBP_CUDA(cudaStreamSynchronize(c->stream));
+                if (c->opt.mapaln && c->h_maperr)
+                    throw Error(CBP_ERR_CUDA, "MAP realignment: a wait between the warps of a pair "
+                                              "timed out");
                 CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
                 c->stage_ms[3] += ms;
                 if (c->opt.mapaln) {

@@ -7,6 +7,16 @@
 
 namespace cbp {
 
+// Phase-2 matrices of a slab are kept in a skewed band layout over the
+// phase-2 column space (the realigned profiles side by side, pass_dst[k]
+// the first column of pair k): cell (r, g) lies in band r/32 at diagonal
+// row g + r%32, lane r%32, so that the 32 cells a warp visits at one step
+// of an anti-diagonal sweep are one contiguous 128-byte row. A band has
+// `nd` = phase-2 positions + 31 diagonal rows; neighbouring pairs share
+// their first and last 31 rows, in disjoint lanes.
+constexpr int kMapMaxWarps = 8;     // warps (32-row bands in flight) per pair
+constexpr int kMapEdgeFields = 6;   // floats per column of a band edge
+
 struct MapArgs {
     const float* scores = nullptr;      // slab score matrix [Lq][ld]
     const float* modscores = nullptr;   // slab modular scores [Lq][ld]
@@ -26,14 +36,25 @@ struct MapArgs {
     const int* pass_idx = nullptr;
     const long long* pass_dst = nullptr;   // phase-2 column of each pair
     float* recs = nullptr;              // [npass][kRecFloats], updated in place
-    float* fb = nullptr;                // [Lq][ld2] forward+backward log MM
-    float* strip = nullptr;             // [5][ld2] band edges
-    uint8_t* btck = nullptr;            // [Lq][ld2] MAP backtrack codes
-    long long ld2 = 0;
+    long long nd = 0;                   // diagonal rows per band
+    float* cs = nullptr;                // [nb][nd][32] cell scores with the pair's offset/multiplier
+    float* fb = nullptr;                // [nb][nd][32] forward, then forward + backward, log MM
+    unsigned* sg = nullptr;             // [nb][nd] bit t: raw score of row 32b+t > 0
+    unsigned long long* bt = nullptr;   // [nb][nd] MAP backtrack codes: bit t | bit 32+t
+    float* strip = nullptr;             // [kMapMaxWarps][6][Ld] band edges per pair, at 48*pass_dst
+    int* err = nullptr;                 // set when a wait between warps gives up
     char* alns = nullptr;               // [5][alnstride] alignment rows
     long long alnstride = 0;
 };
 
+inline long long map_diag_rows(long long npos2) { return npos2 + 31; }
+inline long long map_bands(int Lq) { return (Lq + 31) / 32; }
+inline long long map_strip_floats(long long npos2)
+{
+    return (long long)kMapMaxWarps * kMapEdgeFields * npos2;
+}
+
+// zeroes sg and bt, then realigns every pair of the pass list
 void launch_map(const MapArgs& a, cudaStream_t stream);
 
 }  // namespace cbp

@@ -5,10 +5,9 @@ Several search contexts (slots) share one device copy of the database
 memory and host thread, so the searches of the requests in flight overlap on
 the device. Requests are admitted in arrival order as a slot and enough
 working memory free up: a request's footprint is what its score matrices,
-DP buffers and alignment rows take for one slab of the database,
-``(19 * Lq + 168)`` bytes per slab position (the slab planner's per-position
-cost), with the slab cut so that a request never needs more than
-``max_share`` of the budget. A slot keeps its buffers between requests (they
+DP buffers and alignment rows take for one slab of the database (the slab
+planner's charge, ``cother_b200.slab_bytes``), with the slab cut so that a
+request never needs more than ``max_share`` of the budget. A slot keeps its buffers between requests (they
 only grow), so the ledger charges each slot the largest footprint it has
 held, and admits a request only if the sum over slots stays within the
 budget.
@@ -26,17 +25,23 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-BYTES_PER_CELL = 19           # scores, modular scores, backtrack, phase-2 buffers, rows
-BYTES_PER_POSITION = 168      # per slab position, independent of the query
+def slab_cost(query_len: int, options=None):
+    """(bytes per slab position, bytes per slab) charged for a query."""
+    import cother_b200 as cb
+    fixed = cb.slab_bytes(query_len, 0, options)
+    return cb.slab_bytes(query_len, 1, options) - fixed, fixed
 
 
-def footprint(query_len: int, slab_positions: int) -> int:
-    return (BYTES_PER_CELL * int(query_len) + BYTES_PER_POSITION) * int(slab_positions)
+def footprint(query_len: int, slab_positions: int, options=None) -> int:
+    per_pos, fixed = slab_cost(query_len, options)
+    return fixed + per_pos * int(slab_positions)
 
 
-def slab_positions_for(query_len: int, db_positions: int, budget: int, max_share: float) -> int:
+def slab_positions_for(query_len: int, db_positions: int, budget: int, max_share: float,
+                       options=None) -> int:
     """Largest slab (positions) whose footprint fits max_share of the budget."""
-    cap = int(budget * max_share) // (BYTES_PER_CELL * int(query_len) + BYTES_PER_POSITION)
+    per_pos, fixed = slab_cost(query_len, options)
+    cap = max(0, int(budget * max_share) - fixed) // per_pos
     return max(1, min(int(db_positions), cap))
 
 
@@ -108,6 +113,7 @@ class SearchServer:
                  max_share: float = 0.5, device: int = 0, db_len: int | None = None,
                  n_seqs: int | None = None, run_search=None):
         self.db = db
+        self.options = options
         self._longest = int(np.max(db.lens))   # a slab holds whole profiles
         self.nslots = int(slots)
         self.max_share = float(max_share)
@@ -143,11 +149,11 @@ class SearchServer:
     def submit(self, query) -> Future:
         r = Request(query=query, arrival=time.perf_counter())
         r.slab = slab_positions_for(query.npositions, self.db.npositions, self.ledger.budget,
-                                    self.max_share)
+                                    self.max_share, self.options)
         if r.slab < min(self._longest, self.db.npositions):
             raise ValueError("the memory budget cannot hold one slab of the longest profile "
                              "for this query length")
-        r.need = footprint(query.npositions, r.slab)
+        r.need = footprint(query.npositions, r.slab, self.options)
         with self._cv:
             self._queue.append(r)
             self._cv.notify_all()
@@ -182,15 +188,15 @@ class SearchServer:
                     self._cv.notify_all()
                     return
                 head = self._queue[0]          # first come, first served
-                per_pos = BYTES_PER_CELL * head.query.npositions + BYTES_PER_POSITION
-                i, grant = self.ledger.choose(head.need, per_pos * self._longest)
+                per_pos, fixed = slab_cost(head.query.npositions, self.options)
+                i, grant = self.ledger.choose(head.need, fixed + per_pos * self._longest)
                 if i is None:
                     self._cv.wait()
                     continue
                 self._queue.popleft()
                 if grant < head.need:
-                    head.slab = grant // per_pos
-                    head.need = footprint(head.query.npositions, head.slab)
+                    head.slab = (grant - fixed) // per_pos
+                    head.need = footprint(head.query.npositions, head.slab, self.options)
                 self.ledger.take(i, head.need)
                 self._assigned[i] = head
                 self._cv.notify_all()

@@ -132,6 +132,13 @@ int cbp_share_database(cbp_context* ctx, cbp_context* owner);
  * reference, whose CuDeviceMemory does the same internally). */
 int cbp_device_memory(int device, size_t* free_bytes, size_t* total_bytes);
 
+/* Working device memory that one slab of `positions` database positions
+ * takes for a query of `query_len` positions under `opt`: what the slab
+ * planner charges against a context's budget (the role of the per-chunk
+ * size computation of CuDeviceMemory, src/libmycu/cupro/CuDeviceMemory.cu).
+ * Host-only; needs no device. */
+int cbp_slab_bytes(const cbp_options* opt, size_t query_len, size_t positions, size_t* bytes);
+
 /* Search one query against the resident chunk
  * (CuBatchProcessing::ProcessScoreMatrix, :87-99). `qpmbeg`/`qpmend` are
  * the pointer tables of the query's field arrays (one profile). The call

@@ -78,6 +78,22 @@ def test_map_weak_pairs_and_minpp(oracle_lib, ss_table):
         bp.close()
 
 
+@pytest.mark.parametrize("Lq", [9, 32, 45, 300, 530])
+def test_map_query_lengths(oracle_lib, ss_table, Lq):
+    """Query lengths that give one band (one warp per pair), a last band of
+    a few rows, and more bands than warps (each warp takes several bands);
+    profiles from 1 to 200 positions, shorter and longer than 32 and than
+    the query."""
+    from cother_b200 import synth
+    q = synth.make_profiles([Lq], 300 + Lq, True)
+    db = synth.make_profiles([1, 7, 31, 32, 33, 64, 65, 150, 200, 96], 301 + Lq, False)
+    synth.plant_homologs(q, db, 0.8, seed=302 + Lq)
+    bp = _search(q, db, ss_table, thld=-1.0, logethld=1e9, minpp=0.05)
+    n = _check_map(bp, oracle_lib, q, db, minpp=0.05, logethld=1e9)
+    assert n >= 2
+    bp.close()
+
+
 def test_map_multislab_offsets(oracle_lib, ss_table):
     """Records and alignment rows of several slabs join into one result:
     phase-2 offsets continue across slabs."""
