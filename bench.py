@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--tc", default="plain", choices=["plain", "bf16", "tf32"],
                     help="form of the profile-profile term: FP32 CUDA cores or tensor cores "
                          "(BF16x3 / TF32x3 hi-lo split)")
+    ap.add_argument("--cvswgt", type=float, default=0.0,
+                    help="weight of the context-vector term (0 = off, the parity configuration; "
+                         "the reference's own default is 0.15); > 0 gives the profiles context vectors")
     ap.add_argument("--serve", action="store_true",
                     help="request loop over a resident database: queries/s and p50/p99 latency")
     ap.add_argument("--rate", type=float, default=5.0, help="--serve: offered load (Poisson, queries/s)")
@@ -149,14 +152,14 @@ def measured_peaks():
         return None
 
 
-def oracle_pipeline(q, db, ss, nprof, nthreads, db_len, nseqs):
+def oracle_pipeline(q, db, ss, nprof, nthreads, db_len, nseqs, cvswgt=0.0):
     """The oracle's whole search path (score matrix, phase 1, statistics,
     MAP realignment) for the query against the first `nprof` profiles."""
     from oracle import oracle as O
     import cother_b200 as cb
     db = db.subset(0, nprof)
     ncols = db.npositions
-    sc, ms = O.score_matrix(q, db, ss, ncols=ncols, nthreads=nthreads)
+    sc, ms = O.score_matrix(q, db, ss, ncols=ncols, nthreads=nthreads, cvswgt=cvswgt)
     thld, lthld = cb.score_threshold(q.npositions, db_len)
     sspace, _ = O.length_adjustment(q.npositions, db_len, nseqs)
     rec, _ = O.dp1(q, db, sc, 0, 0, nprof, thld)
@@ -169,7 +172,7 @@ def oracle_pipeline(q, db, ss, nprof, nthreads, db_len, nseqs):
     return ncols
 
 
-def cpu_baseline(q, db, ss, seconds: float, db_len: int, nseqs: int):
+def cpu_baseline(q, db, ss, seconds: float, db_len: int, nseqs: int, cvswgt: float = 0.0):
     """Oracle (a port of the reference kernels) on the host cores, on a
     bounded sample: the query against the first database profiles, through
     the whole path."""
@@ -177,13 +180,13 @@ def cpu_baseline(q, db, ss, seconds: float, db_len: int, nseqs: int):
     # calibrate on a few profiles, then size the timed sample
     probe = min(db.nprofiles, 4)
     t = time.perf_counter()
-    cols = oracle_pipeline(q, db, ss, probe, ncpu, db_len, nseqs)
+    cols = oracle_pipeline(q, db, ss, probe, ncpu, db_len, nseqs, cvswgt)
     dt = max(time.perf_counter() - t, 1e-3)
     rate = cols / dt
     mean_len = float(db.lens.mean())
     nprof = int(min(db.nprofiles, max(probe, rate * seconds / mean_len)))
     t = time.perf_counter()
-    cols = oracle_pipeline(q, db, ss, nprof, ncpu, db_len, nseqs)
+    cols = oracle_pipeline(q, db, ss, nprof, ncpu, db_len, nseqs, cvswgt)
     dt = time.perf_counter() - t
     cells = q.npositions * cols
     return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": ncpu, "kind": "port",
@@ -201,12 +204,13 @@ def run_reference(args):
     from cother_b200 import synth
     ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
     ndb = args.ndb or 200
-    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=ndb)
+    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=ndb,
+                                context_vectors=args.cvswgt > 0)
     vals = []
     full = synth.db_lengths(args.workload, args.seed)
     db_len, nseqs = int(full.sum()), len(full)
     for _ in range(max(1, args.warmup) + args.steps):
-        vals.append(cpu_baseline(q, db, ss, args.cpu_seconds / 3, db_len, nseqs))
+        vals.append(cpu_baseline(q, db, ss, args.cpu_seconds / 3, db_len, nseqs, args.cvswgt))
     timed = vals[-args.steps:] if args.steps > 0 else vals
     v = float(np.mean([x["value"] for x in timed]))
     cb = dict(timed[-1])
@@ -214,7 +218,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "stages": STAGES},
+            "config": {"workload": args.workload, "stages": STAGES, "cvswgt": args.cvswgt},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -282,13 +286,17 @@ def main():
     ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
     # one query for all ranks; each rank holds its own database shard
     q, db = synth.make_workload(args.workload, seed=args.seed, ndb=args.ndb,
-                                db_seed=args.seed + 1000 * rank)
+                                db_seed=args.seed + 1000 * rank, context_vectors=args.cvswgt > 0)
     Lq, Ndb = q.npositions, db.npositions
     steps_ddms = total_ddms_steps(q, db)
 
     opts = cb.Options.defaults()
     opts.tc_form = {"plain": cb.TC_PLAIN, "bf16": cb.TC_BF16X3, "tf32": cb.TC_TF32X3}[args.tc]
+    opts.cvswgt = args.cvswgt
     bp = cb.BatchProcessing(ss, opts, device=local)
+    if args.cvswgt > 0:
+        cvs = np.load(os.path.join(ROOT, "tests", "golden", "cvs2s.npz"))
+        bp.set_cvs2s_map(cvs["keys"], cvs["scores"])
     bp.transfer_cpm_data(db)
     db_len, nseqs = Ndb * world, db.nprofiles * world
     bp.set_db_details(db_len, nseqs)
@@ -369,6 +377,7 @@ def main():
                 "dtype": "f32", "data": "synthetic",
                 "config": {"workload": args.workload, "query_len": Lq, "db_profiles": db.nprofiles,
                            "db_positions": Ndb, "stages": STAGES, "tc_form": args.tc,
+                           "cvswgt": args.cvswgt,
                            "l2": "inputs larger than L2 (database chunk > 126 MB)",
                            "parallelism": f"dp{world} (database shard per GPU)"},
                 "e2e": {"value": e2e, "unit": "GCUPS",
@@ -381,7 +390,7 @@ def main():
                 "stage_ms": {k: v / steps for k, v in zip(STAGES, stage_acc)},
                 "gpu_launches": launches, "roofline": roof, "clocks": clocks}
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds, db_len, nseqs)
+            line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds, db_len, nseqs, args.cvswgt)
         print(json.dumps(line))
     bp.close()
     if dist is not None:

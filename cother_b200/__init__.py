@@ -73,6 +73,7 @@ def load_library(path: str | None = None):
         "cbp_set_query_len": (i32, [vp, sz]),
         "cbp_set_score_threshold": (i32, [vp, f32]),
         "cbp_set_logE_threshold": (i32, [vp, f32]),
+        "cbp_set_cvs2s_map": (i32, [vp, vp, vp, sz]),
         "cbp_transfer_chunk": (i32, [vp, vp, vp, vp]),
         "cbp_process": (i32, [vp, i32, sz, vp, vp]),
         "cbp_wait_idle": (i32, [vp]),
@@ -209,6 +210,16 @@ class BatchProcessing:
 
     def set_logE_threshold(self, t: float) -> None:
         _check(load_library().cbp_set_logE_threshold(self._h, float(t)))
+
+    def set_cvs2s_map(self, keys, scores) -> None:
+        """The context-vector score map, needed when CVSWGT > 0: keys on the
+        grid of halves and their scores, as the reference's CVS2Scores
+        reader leaves them (smoothed)."""
+        k = np.ascontiguousarray(keys, np.float32)
+        v = np.ascontiguousarray(scores, np.float32)
+        if k.shape != v.shape or k.ndim != 1:
+            raise ValueError("keys and scores must be 1-D arrays of equal length")
+        _check(load_library().cbp_set_cvs2s_map(self._h, k.ctypes.data, v.ctypes.data, len(k)))
 
     def set_max_slab_positions(self, n: int) -> None:
         _check(load_library().cbp_set_max_slab_positions(self._h, int(n)))

@@ -126,7 +126,7 @@ struct DevBuf {
 
 // Device copy of a packed profile set.
 struct ProfilesStore {
-    DevBuf tf, ss, dst, dstlen, trn, bkg, eno, plen, pstart, pro, aa, sss;
+    DevBuf tf, ss, dst, dstlen, trn, bkg, eno, plen, pstart, pro, aa, sss, cv, cvprior, cvnorm2;
     ProfilesDev view;
     std::vector<int> h_plen;
     std::vector<long long> h_pstart;
@@ -135,7 +135,8 @@ struct ProfilesStore {
     ProfilesStore& operator=(const ProfilesStore&) = delete;
     ~ProfilesStore() { release(); }
     void release() {
-        for (DevBuf* b : {&tf, &ss, &dst, &dstlen, &trn, &bkg, &eno, &plen, &pstart, &pro, &aa, &sss})
+        for (DevBuf* b : {&tf, &ss, &dst, &dstlen, &trn, &bkg, &eno, &plen, &pstart, &pro, &aa, &sss,
+                          &cv, &cvprior, &cvnorm2})
             b->release();
         view = ProfilesDev();
         h_plen.clear();
@@ -174,6 +175,11 @@ struct cbp_context {
     float ref_lambda = 1.116276f, ref_K = 0.115812f;
     float gap_lambda = 0.561132f, gap_K = 0.001488f, gap_alpha = 0.5f, gap_beta = -1.0f;
     DevBuf nnweights;
+    // context-vector score map (cbp_set_cvs2s_map)
+    DevBuf cvsmap;
+    bool have_cvs = false;
+    int cvs_card = 0, cvs_shift = 0;
+    float cvs_key_first = 0.f, cvs_key_last = 0.f;
     // working buffers
     DevBuf scores, modscores, btck, bandbuf, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
     DevBuf hitrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf;
@@ -242,7 +248,10 @@ size_t field_bytes(char* const* beg, char* const* end, int f)
 }
 
 // Repack 181 SoA host fields into the device layout (layout.h) and upload.
-void upload_profiles(ProfilesStore& st, char* const* beg, char* const* end, cudaStream_t stream)
+// Upload a packed profile set. With `with_cv` the context-vector fields
+// (pmv2DCVentrs.., pmv2DCVprior, pmv2DCVnorm2) are uploaded too.
+void upload_profiles(ProfilesStore& st, char* const* beg, char* const* end, cudaStream_t stream,
+                     bool with_cv)
 {
     if (!beg || !end) throw Error(CBP_ERR_ARG, "null field tables");
     const size_t P = field_bytes(beg, end, fLen) / sizeof(int);
@@ -259,6 +268,10 @@ void upload_profiles(ProfilesStore& st, char* const* beg, char* const* end, cuda
     for (int s = 0; s < 100; s++)
         if (field_bytes(beg, end, fDD + s) != N * sizeof(float))
             throw Error(CBP_ERR_ARG, "distance fields of unequal size");
+    if (with_cv)
+        for (int k = 0; k < kNCV + 2; k++)
+            if (field_bytes(beg, end, fCV + k) != N * sizeof(float))
+                throw Error(CBP_ERR_ARG, "context-vector fields missing or of unequal size");
     const int* lens = reinterpret_cast<const int*>(beg[fLen]);
     const uint32_t* dists = reinterpret_cast<const uint32_t*>(beg[fDist]);
     st.h_plen.assign(lens, lens + P);
@@ -334,6 +347,11 @@ void upload_profiles(ProfilesStore& st, char* const* beg, char* const* end, cuda
     up(st.sss, beg[fSSstate], N);
     up(st.dst, dst.data(), dst.size());
     up(st.dstlen, dlen.data(), N);
+    if (with_cv) {
+        up_rows(st.cv, fCV, kNCV, N, sizeof(float));
+        up(st.cvprior, beg[fCV + kNCV], N * sizeof(float));
+        up(st.cvnorm2, beg[fCV + kNCV + 1], N * sizeof(float));
+    }
     CBP_CUDA(cudaStreamSynchronize(stream));
 
     ProfilesDev& v = st.view;
@@ -343,6 +361,9 @@ void upload_profiles(ProfilesStore& st, char* const* beg, char* const* end, cuda
     v.trn = st.trn.as<float>(); v.bkg = st.bkg.as<float>(); v.eno = st.eno.as<float>();
     v.plen = st.plen.as<int>(); v.pstart = st.pstart.as<long long>();
     v.pro = st.pro.as<int>(); v.aa = st.aa.as<int8_t>(); v.sss = st.sss.as<int8_t>();
+    v.cv = with_cv ? st.cv.as<float>() : nullptr;
+    v.cvprior = with_cv ? st.cvprior.as<float>() : nullptr;
+    v.cvnorm2 = with_cv ? st.cvnorm2.as<float>() : nullptr;
 }
 
 void check_ctx(cbp_context* c)
@@ -373,6 +394,25 @@ size_t slab_bytes_per_position(const cbp_options& o, int Lq)
 size_t slab_fixed_bytes(int Lq)
 {
     return 31 * (size_t)map_bands(Lq) * (8 * 32 + 12);
+}
+
+// Constants of the context-vector score (_TCTXVECT::_TCTXVECT,
+// src/libpro/srcpro/TCTXVECT.cpp:26-60), computed in float with the host's
+// logf as the reference does: dimension 19, kappa0 0.1, nu0 19;
+// 1/kappa0, -(nu0+2)/2 and (dim/2 - (nu0+2)/2) (ln kappa0 - ln(kappa0+2))
+// + sum_{i=1..dim} (ln(nu0+1-i) - ln 2).
+void cvs_constants(float* lokappa0, float* pownu0, float* cterm)
+{
+    const int dim = 19;
+    const float kappa0 = 0.1f, nu0 = (float)dim;
+    const float pw = -0.5f * (nu0 + 2.f);
+    float ct = (0.5f * dim + pw) * (logf(kappa0) - logf(kappa0 + 2.f));
+    float sum = 0.0f;
+    for (int i = 1; i <= dim; i++) sum += logf(nu0 + 1.0f - i) - 0.69314718055994530942f;
+    ct += sum;
+    *lokappa0 = 1.f / kappa0;
+    *pownu0 = pw;
+    *cterm = ct;
 }
 
 // Slabs of whole profiles whose score matrices fit the working budget.
@@ -435,8 +475,8 @@ int cbp_create(int device, const cbp_options* opt, const float* ss_table, size_t
         if (!out) throw Error(CBP_ERR_ARG, "null output pointer");
         *out = nullptr;
         if (!opt || !ss_table) throw Error(CBP_ERR_ARG, "null options or SS table");
-        if (opt->cvswgt != 0.0f)
-            throw Error(CBP_ERR_ARG, "CVSWGT > 0 (context-vector term) is not supported");
+        if (!(opt->cvswgt >= 0.0f && opt->cvswgt < 1.0f))
+            throw Error(CBP_ERR_ARG, "CVSWGT must be in [0, 1)");
         // value ranges of src/libpro/srcpro/MOptions.cpp:76-141
         if (!(opt->ssswgt >= 0.0f && opt->ssswgt < 1.0f))
             throw Error(CBP_ERR_ARG, "SSSWGT must be in [0,1)");
@@ -487,7 +527,8 @@ int cbp_destroy(cbp_context* c)
     c->query.release();
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax, &c->dpcoords,
                       &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
-                      &c->cs2, &c->fb2, &c->sg2, &c->bt2, &c->strip2, &c->maperr, &c->alnbuf})
+                      &c->cs2, &c->fb2, &c->sg2, &c->bt2, &c->strip2, &c->maperr, &c->alnbuf,
+                      &c->cvsmap})
         b->release();
     c->sstab.release();
     c->dmstab.release();
@@ -532,7 +573,7 @@ int cbp_transfer_chunk(cbp_context* c, char* const* beg, char* const* end, const
         c->have_db = false;
         // a fresh store: contexts sharing the previous one keep it
         auto st = std::make_shared<ProfilesStore>();
-        upload_profiles(*st, beg, end, c->stream);
+        upload_profiles(*st, beg, end, c->stream, c->opt.cvswgt > 0.0f);
         c->db = std::move(st);
         c->have_db = true;
     });
@@ -574,13 +615,47 @@ int cbp_share_database(cbp_context* c, cbp_context* owner)
     });
 }
 
+int cbp_set_cvs2s_map(cbp_context* c, const float* keys, const float* scores, size_t card)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!keys || !scores) throw Error(CBP_ERR_ARG, "null keys or scores");
+        if (card < 1 || card > 100000) throw Error(CBP_ERR_ARG, "invalid map cardinality");
+        // the lookup (SerializedCVS2Scores::GetScoreE1S1Step2Boundary) indexes
+        // the scores by shift + rint(2 x score): keys must be the halves
+        // (i - shift)/2, shift the number of negative keys
+        int shift = 0;
+        while ((size_t)shift < card && keys[shift] < 0.0f) shift++;
+        for (size_t i = 0; i < card; i++)
+            if (keys[i] != 0.5f * (float)((long long)i - shift))
+                throw Error(CBP_ERR_ARG, "CVS map keys must be consecutive halves");
+        for (size_t i = 0; i < card; i++)
+            if (!std::isfinite(scores[i])) throw Error(CBP_ERR_ARG, "non-finite CVS map score");
+        CBP_CUDA(cudaSetDevice(c->device));
+        c->cvsmap.reserve(card * sizeof(float));
+        CBP_CUDA(cudaMemcpy(c->cvsmap.p, scores, card * sizeof(float), cudaMemcpyHostToDevice));
+        c->cvs_card = (int)card;
+        c->cvs_shift = shift;
+        c->cvs_key_first = keys[0];
+        c->cvs_key_last = keys[card - 1];
+        c->have_cvs = true;
+    });
+}
+
 int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* const* qbeg,
                 char* const* qend)
 {
     return guarded([&] {
         check_ctx(c);
         if (!c->have_db) throw Error(CBP_ERR_STATE, "no database chunk transferred");
-        upload_profiles(c->query, qbeg, qend, c->stream);
+        if (c->opt.cvswgt > 0.0f) {
+            if (!c->have_cvs)
+                throw Error(CBP_ERR_STATE, "CVSWGT > 0 needs the context-vector map (cbp_set_cvs2s_map)");
+            if (!c->db->view.cv)
+                throw Error(CBP_ERR_STATE, "CVSWGT > 0 needs a database chunk with context vectors "
+                                           "(transferred by a context with CVSWGT > 0)");
+        }
+        upload_profiles(c->query, qbeg, qend, c->stream, c->opt.cvswgt > 0.0f);
         const int Lq = (int)c->query.view.N;
         if (c->query.view.P != 1) throw Error(CBP_ERR_ARG, "the query field tables must hold one profile");
         if ((size_t)Lq != query_len) throw Error(CBP_ERR_ARG, "query_len differs from the query profile length");
@@ -639,6 +714,15 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             a.ddmswgt = c->opt.ddmswgt;
             a.initshift = c->opt.mapaln ? 0.002f : 0.0003f;
             a.dstsegm = c->opt.dstsegm;
+            if (c->opt.cvswgt > 0.0f) {
+                a.cvswgt = c->opt.cvswgt;
+                a.cvs_scores = c->cvsmap.as<float>();
+                a.cvs_card = c->cvs_card;
+                a.cvs_shift = c->cvs_shift;
+                a.cvs_key_first = c->cvs_key_first;
+                a.cvs_key_last = c->cvs_key_last;
+                cvs_constants(&a.cvs_lokappa0, &a.cvs_pownu0, &a.cvs_cterm);
+            }
             a.sstab = c->sstab.as<float>();
             a.dmstab = c->dmstab.as<float>();
             a.scores = c->scores.as<float>();

@@ -22,6 +22,7 @@
 namespace cbp {
 
 constexpr int kNAA = 20;
+constexpr int kNCV = 19;          // context-vector entries (pmv2DNoCVEls)
 constexpr int kNSS = 3;
 constexpr int kNTrn = 7;
 constexpr int kMaxDst = 99;
@@ -48,6 +49,11 @@ struct ProfilesDev {
     const int* pro = nullptr;
     const int8_t* aa = nullptr;
     const int8_t* sss = nullptr;
+    // context vectors, when uploaded: [19][N] entries, [N] log priors, [N]
+    // squared norms
+    const float* cv = nullptr;
+    const float* cvprior = nullptr;
+    const float* cvnorm2 = nullptr;
 };
 
 }  // namespace cbp

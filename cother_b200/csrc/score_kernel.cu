@@ -182,6 +182,32 @@ __device__ __forceinline__ float ddms_cell(const uint8_t* __restrict__ q, int le
     return sum * 128.0f;
 }
 
+// Context-vector term of one cell (CalcCVS2ScoreSMEMUnroll2x,
+// src/libmycu/cusco/CuBatchScoreMatrix_cvs2s.cuh:47-136): the log-odds of
+// the two normal vectors, log det(C2 + H'H) from their dot product and
+// squared norms less both log priors, translated through the map
+// (SerializedCVS2Scores::GetScoreE1S1Step2Boundary,
+// src/libmycu/cupro/SerializedCVS2Scores.cuh:377-410). The dot product, the
+// determinant and the log-odds are fused multiply-adds and the logarithm is
+// the __logf intrinsic, as in the reference's build. A log-odds that is
+// not above the first key (a NaN included) takes the first score.
+__device__ __forceinline__ float cvs_cell(const ScoreArgs& a, const float* __restrict__ qcv, float qprior,
+                                          float qnorm2, const float (*__restrict__ dcv)[kCols], int lane,
+                                          float dprior, float dnorm2)
+{
+    float dot = 0.0f;
+#pragma unroll
+    for (int i = 0; i < kNCV; i++) dot = __fmaf_rn(qcv[i], dcv[i][lane], dot);
+    dot = dot + a.cvs_lokappa0;
+    const float qa = qnorm2 + 1.0f + a.cvs_lokappa0;
+    const float da = dnorm2 + 1.0f + a.cvs_lokappa0;
+    const float det = __fmaf_rn(qa, da, -(dot * dot));
+    const float lo = __fmaf_rn(a.cvs_pownu0, __logf(det), a.cvs_cterm) - qprior - dprior;
+    if (!(a.cvs_key_first < lo)) return __ldg(a.cvs_scores);
+    if (a.cvs_key_last <= lo) return __ldg(a.cvs_scores + a.cvs_card - 1);
+    return __ldg(a.cvs_scores + a.cvs_shift + (int)rintf(lo + lo));
+}
+
 __global__ void __launch_bounds__(kThreads)
 score_matrix_kernel(const ScoreArgs a)
 {
@@ -197,6 +223,10 @@ score_matrix_kernel(const ScoreArgs a)
     __shared__ float s_qbg[kNAA];
     __shared__ int s_dlen[kCols];
     __shared__ int s_qlen[kRows];
+    __shared__ float s_dcv[kNCV][kCols];      // context vectors (CVSWGT > 0)
+    __shared__ float s_dcvpn[2][kCols];       // their log priors and squared norms
+    __shared__ float s_qcv[kRows][kNCV + 1];
+    __shared__ float s_qcvpn[2][kRows];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -248,6 +278,25 @@ score_matrix_kernel(const ScoreArgs a)
         const int row = rowb + r;
         s_qss[r][k] = row < a.Lq ? a.q.ss[(long long)k * a.q.N + row] : 0.0f;
     }
+    if (a.cvswgt > 0.0f) {
+        if (cvalid) {
+            for (int k = warp; k < kNCV; k += kWarps) s_dcv[k][lane] = a.db.cv[(long long)k * N + gpos];
+            if (warp == 0) {
+                s_dcvpn[0][lane] = a.db.cvprior[gpos];
+                s_dcvpn[1][lane] = a.db.cvnorm2[gpos];
+            }
+        }
+        for (int idx = tid; idx < kRows * kNCV; idx += kThreads) {
+            const int r = idx / kNCV, k = idx - r * kNCV;
+            const int row = rowb + r;
+            s_qcv[r][k] = row < a.Lq ? a.q.cv[(long long)k * a.q.N + row] : 0.0f;
+        }
+        if (tid < kRows) {
+            const int row = rowb + tid;
+            s_qcvpn[0][tid] = row < a.Lq ? a.q.cvprior[row] : 0.0f;
+            s_qcvpn[1][tid] = row < a.Lq ? a.q.cvnorm2[row] : 0.0f;
+        }
+    }
     if (tid < kNAA) s_qbg[tid] = a.q.bkg[tid];
     if (tid < kRows) s_qlen[tid] = (rowb + tid < a.Lq) ? a.q.dstlen[rowb + tid] : 0;
     for (int idx = tid; idx < kRows * (kElems / 4); idx += kThreads) {
@@ -283,6 +332,10 @@ score_matrix_kernel(const ScoreArgs a)
         }
         float s = cb_logf(acc) - a.initshift;
         float mod = 0.0f;
+        const float cvs = (a.cvswgt > 0.0f)
+                              ? cvs_cell(a, s_qcv[r], s_qcvpn[0][r], s_qcvpn[1][r], s_dcv, lane,
+                                         s_dcvpn[0][lane], s_dcvpn[1][lane])
+                              : 0.0f;
 
         // SS term (CuBatchScoreMatrix_ssss.cu:209-279)
         if (a.ssswgt > 0.0f) {
@@ -304,8 +357,24 @@ score_matrix_kernel(const ScoreArgs a)
                 ss = ss - 0.05f;
                 ss = ss * a.ssswgt;
             }
-            s = s + ss;
-            mod = ss;
+            if (a.cvswgt > 0.0f) {
+                // SS plus the weighted CVS term, the modular score 0.5*CVSWGT
+                // lower (CuBatchScoreMatrix_ssss_cvs2s.cu:252-270). That
+                // kernel computes chunk columns c and c+32 of each 64-column
+                // block in one thread, and its build fuses the addition for
+                // the first (one rounding) but not for the second.
+                ss = ((gpos >> 5) & 1) ? ss + cvs * a.cvswgt : __fmaf_rn(cvs, a.cvswgt, ss);
+                s = s + ss;
+                mod = ss - 0.5f * a.cvswgt;
+            } else {
+                s = s + ss;
+                mod = ss;
+            }
+        } else if (a.cvswgt > 0.0f && cvs != 0.0f) {
+            // CVS alone (CuBatchScoreMatrix_cvs2s.cu:286-299); the modular
+            // score starts at zero
+            s = s + cvs * a.cvswgt;
+            mod = mod + (cvs - 0.5f) * a.cvswgt;
         }
 
         // DDMS term (CuBatchScoreMatrix_ddms2s_h2.cu:158-186)

@@ -15,6 +15,13 @@ struct ScoreArgs {
     int Lq = 0;
     float ssswgt = 0.f, ddmswgt = 0.f, initshift = 0.f;
     int dstsegm = 6;
+    // context-vector term (CVSWGT > 0): the map's scores for keys
+    // (i - cvs_shift)/2, its first and last keys, and the score's constants
+    float cvswgt = 0.f;
+    const float* cvs_scores = nullptr;
+    int cvs_card = 0, cvs_shift = 0;
+    float cvs_key_first = 0.f, cvs_key_last = 0.f;
+    float cvs_lokappa0 = 0.f, cvs_pownu0 = 0.f, cvs_cterm = 0.f;
     const float* sstab = nullptr;   // [30][30]
     const float* dmstab = nullptr;  // [22][22]
     float* scores = nullptr;        // [Lq][ld]

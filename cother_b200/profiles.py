@@ -83,6 +83,11 @@ class ProfileSet:
     aa: np.ndarray
     ssstate: np.ndarray
     names: list = field(default_factory=list)
+    # context vectors (optional): [19][N] entries, their prior log
+    # probabilities and squared norms [N]; zeros are passed when absent
+    cv: np.ndarray | None = None
+    cvprior: np.ndarray | None = None
+    cvnorm2: np.ndarray | None = None
     _keep: list = field(default_factory=list, repr=False)
 
     def __post_init__(self):
@@ -122,6 +127,9 @@ class ProfileSet:
             aa=self.aa[s0:s0 + n].copy(),
             ssstate=self.ssstate[s0:s0 + n].copy(),
             names=list(self.names[first:first + count]) if self.names else [],
+            cv=None if self.cv is None else np.ascontiguousarray(self.cv[:, s0:s0 + n]),
+            cvprior=None if self.cvprior is None else self.cvprior[s0:s0 + n].copy(),
+            cvnorm2=None if self.cvnorm2 is None else self.cvnorm2[s0:s0 + n].copy(),
         )
 
     def field_tables(self):
@@ -150,10 +158,16 @@ class ProfileSet:
             put(PTR_TRNPRBS + t, self.trn[t], 4 * (N + P))
         for a in range(NUMAA):
             put(PMV_TRGFRQS + a, self.tf[a], 4 * N)
-        for c in range(NCVELS):
-            put(PMV_CVENTRS + c, z, 4 * N)
-        put(PMV_CVPRIOR, z, 4 * N)
-        put(PMV_CVNORM2, z, 4 * N)
+        if self.cv is not None:
+            for c in range(NCVELS):
+                put(PMV_CVENTRS + c, self.cv[c], 4 * N)
+            put(PMV_CVPRIOR, self.cvprior, 4 * N)
+            put(PMV_CVNORM2, self.cvnorm2, 4 * N)
+        else:
+            for c in range(NCVELS):
+                put(PMV_CVENTRS + c, z, 4 * N)
+            put(PMV_CVPRIOR, z, 4 * N)
+            put(PMV_CVNORM2, z, 4 * N)
         for s in range(NDSTSLOTS):
             put(PMV_DDVALUES + s, self.dd[s], 4 * N)
         for s in range(NSSSTATES):

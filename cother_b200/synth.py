@@ -125,7 +125,41 @@ def plant_homologs(query: ProfileSet, db: ProfileSet, fraction: float, seed: int
         db.dd[:, s0:s0 + n] = dl
         db.aa[s0:s0 + n] = query.aa[qa:qa + n]
         db.ssstate[s0:s0 + n] = query.ssstate[qa:qa + n]
+        if query.cv is not None and db.cv is not None:
+            db.cv[:, s0:s0 + n] = (np.float32(w) * query.cv[:, qa:qa + n] +
+                                   np.float32(noise) * db.cv[:, s0:s0 + n])
+            db.cvnorm2[s0:s0 + n], db.cvprior[s0:s0 + n] = cv_magnitudes(db.cv[:, s0:s0 + n])
     return picks
+
+
+# normal-Wishart prior of context vectors (src/libpro/srcpro/TCTXVECT.cpp:26-60):
+# dimension 19, kappa0 0.1, nu0 19; the log prior of a vector is
+# LPFACT - (nu0+1)/2 * log(1 + kappa0/(kappa0+1) * |v|^2)
+# (src/libpro/srcpro/PMProfileModel.cpp:363-387, 823-828), with LPFACT =
+# lgamma(10) - lgamma(1/2) + 19/2 * (log 0.1 - log 1.1)
+CV_DIM = 19
+CV_LPFACT = np.float32(-10.550543)
+
+
+def cv_magnitudes(cv: np.ndarray):
+    """(squared norms, log prior probabilities) of context vectors [19][n]."""
+    cv = np.asarray(cv, np.float32)
+    norm2 = np.zeros(cv.shape[1], np.float32)
+    for d in range(cv.shape[0]):
+        norm2 = norm2 + cv[d] * cv[d]
+    prior = CV_LPFACT - np.float32(10.0) * np.log(np.float32(1.0) + np.float32(0.1 / 1.1) * norm2)
+    return norm2, prior.astype(np.float32)
+
+
+def add_context_vectors(ps: ProfileSet, seed: int) -> ProfileSet:
+    """Give every position of `ps` a context vector: 19 standard normal
+    entries (a stand-in for the reference profile builder's mixed
+    logit-normal transform of the target frequencies), with its squared norm
+    and log prior probability. Seeded apart from the other fields."""
+    rng = np.random.default_rng([int(seed) & 0xFFFFFFFF, 0xC5])
+    ps.cv = rng.standard_normal((CV_DIM, ps.npositions), dtype=np.float32)
+    ps.cvnorm2, ps.cvprior = cv_magnitudes(ps.cv)
+    return ps
 
 
 def lognormal_lengths(n: int, median: float, lo: int, hi: int, seed: int,
@@ -178,16 +212,21 @@ HOMOLOG_FRACTION = 0.01
 
 
 def make_workload(name: str, seed: int = 7, ndb: int | None = None, qindex: int = 0,
-                  homologs: float = HOMOLOG_FRACTION, db_seed: int | None = None):
+                  homologs: float = HOMOLOG_FRACTION, db_seed: int | None = None,
+                  context_vectors: bool = False):
     """(query ProfileSet, database ProfileSet) for a named workload; a
     fraction `homologs` of the database profiles are planted homologs of
     the query. The query depends on `seed` only; the database on `db_seed`
-    (default `seed`), so that shards of one search can share the query."""
+    (default `seed`), so that shards of one search can share the query.
+    With `context_vectors`, both sides carry context vectors (the CVS term)."""
     w = WORKLOADS[name]
     dseed = seed if db_seed is None else db_seed
     lens = db_lengths(name, dseed, ndb)
     db = make_profiles(lens, seed=dseed * 1000 + 1, predicted=False, window=w["window"])
     q = make_profiles([w["qlens"][qindex]], seed=seed * 1000 + 2 + qindex, predicted=True,
                       window=w["window"])
+    if context_vectors:
+        add_context_vectors(db, dseed * 1000 + 1)
+        add_context_vectors(q, seed * 1000 + 2 + qindex)
     plant_homologs(q, db, homologs, seed=dseed * 1000 + 3 + qindex)
     return q, db

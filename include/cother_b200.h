@@ -57,7 +57,9 @@ typedef struct cbp_context cbp_context;
 
 typedef struct cbp_options {
     float ssswgt;     /* SSSWGT: weight of the SS score, [0,1) */
-    float cvswgt;     /* CVSWGT: context-vector term; must be 0 (term off) */
+    float cvswgt;     /* CVSWGT: weight of the context-vector term, [0,1); > 0 needs
+                       * cbp_set_cvs2s_map and context vectors in the profiles
+                       * (the reference's own default is 0.15) */
     float ddmswgt;    /* DDMSWGT: weight of the DDMS score */
     int   dstsegm;    /* DSTSEGM: minimum DDMS segment length */
     int   mapaln;     /* MAPALN: 1 = MAP realignment in phase 2 */
@@ -131,6 +133,16 @@ int cbp_share_database(cbp_context* ctx, cbp_context* owner);
  * callers that divide it between contexts (no counterpart in the
  * reference, whose CuDeviceMemory does the same internally). */
 int cbp_device_memory(int device, size_t* free_bytes, size_t* total_bytes);
+
+/* The context-vector score map (the reference's CVS2Scores, read from
+ * src/env/cvs2s and handed to CuDeviceMemory::CacheCVS2Scores,
+ * src/libmycu/cupro/CuDeviceMemory.cu:214-219, 691-740): `card` keys on the
+ * grid of halves (keys[i] = (i - s)/2 with s the number of negative keys)
+ * and their scores, as the reference's reader leaves them (smoothed). It
+ * is required before cbp_process when CVSWGT > 0; the database and query
+ * profiles then need their context-vector fields (pmv2DCVentrs,
+ * pmv2DCVprior, pmv2DCVnorm2). */
+int cbp_set_cvs2s_map(cbp_context* ctx, const float* keys, const float* scores, size_t card);
 
 /* Working device memory that one slab of `positions` database positions
  * takes for a query of `query_len` positions under `opt`: what the slab

@@ -281,6 +281,65 @@ static float orc_ss_score(const float* qss, long long qstride, const float* dss,
     return acc;
 }
 
+/* Context-vector score constants (_TCTXVECT::_TCTXVECT,
+ * src/libpro/srcpro/TCTXVECT.cpp:26-60): dimension 19, kappa0 0.1, nu0 19;
+ * lokappa0 = 1/kappa0, pownu0 = -(nu0+2)/2 and
+ * cterm = (dim/2 + pownu0)(ln kappa0 - ln(kappa0+2)) + sum_{i=1..dim} (ln(nu0+1-i) - ln 2),
+ * in float with the C library's logf as the reference's host code. */
+void orc_cvs_constants(float* lokappa0, float* pownu0, float* cterm)
+{
+    const int dim = 19;
+    const float kappa0 = 0.1f;
+    const float nu0 = (float)dim;
+    const float pw = -0.5f * (nu0 + 2.f);
+    float ct = (0.5f * dim + pw) * (logf(kappa0) - logf(kappa0 + 2.f));
+    float sum = 0.0f;
+    for (int i = 1; i <= dim; i++) sum += logf(nu0 + 1.0f - i) - 0.69314718055994530941723212146f;
+    ct += sum;
+    *lokappa0 = 1.f / kappa0;
+    *pownu0 = pw;
+    *cterm = ct;
+}
+
+float orc_cvs_lookup(const orc_score_params* prm, float lo)
+{
+    if (!(prm->cvs_key_first < lo)) return prm->cvs_scores[0];   /* NaN too */
+    if (prm->cvs_key_last <= lo) return prm->cvs_scores[prm->cvs_card - 1];
+    return prm->cvs_scores[prm->cvs_shift + (int)rintf(lo + lo)];
+}
+
+/* The map value of cell (r, c) (CalcCVS2ScoreSMEMUnroll2x,
+ * src/libmycu/cusco/CuBatchScoreMatrix_cvs2s.cuh:47-136): the log-odds of
+ * the two normal vectors, log det(C2 + H'H) from their dot product and
+ * squared norms, less both log priors, translated through the map. The dot
+ * product, the determinant and the log-odds are contracted into fused
+ * multiply-adds as the reference's CUDA build does. The reference takes the logarithm with
+ * the fast intrinsic __logf (at most 3 ulp from the true value here, since
+ * the determinant is at least 21); this restatement uses logf, and flags
+ * the cell when the lookup would change within 8 ulp of the logarithm. */
+static float orc_cvs_cell(const orc_score_params* prm, long long r, long long Lq, long long c,
+                          long long N, float lokappa0, float pownu0, float cterm, int* ambiguous)
+{
+    float dot = 0.0f;
+    for (int i = 0; i < 19; i++)
+        dot = fmaf(prm->q_cv[i * Lq + r], prm->d_cv[i * N + c], dot);
+    dot = dot + lokappa0;
+    const float a = prm->q_cvnorm2[r] + 1.0f + lokappa0;
+    const float b = prm->d_cvnorm2[c] + 1.0f + lokappa0;
+    const float det = fmaf(a, b, -(dot * dot));
+    const float lg = logf(det);
+    const float qp = prm->q_cvprior[r], dp = prm->d_cvprior[c];
+    const float lo = fmaf(pownu0, lg, cterm) - qp - dp;
+    const float v = orc_cvs_lookup(prm, lo);
+    if (ambiguous) {
+        const float d8 = 8.0f * (nextafterf(fabsf(lg), INFINITY) - fabsf(lg));
+        const float lo1 = fmaf(pownu0, lg - d8, cterm) - qp - dp;
+        const float lo2 = fmaf(pownu0, lg + d8, cterm) - qp - dp;
+        *ambiguous = orc_cvs_lookup(prm, lo1) != v || orc_cvs_lookup(prm, lo2) != v;
+    }
+    return v;
+}
+
 void orc_score_matrix(int Lq, const float* q_tf, const float* q_bkg, const float* q_ss,
                       const uint8_t* q_dd,
                       long long N, int P, const float* d_tf, const float* d_bkg,
@@ -289,15 +348,41 @@ void orc_score_matrix(int Lq, const float* q_tf, const float* q_bkg, const float
                       long long col0, long long ncols,
                       float* scores, float* modscores, long long ld)
 {
+    float lokappa0 = 0.f, pownu0 = 0.f, cterm = 0.f;
+    const int cvs = prm->cvswgt > 0.0f;
+    if (cvs) orc_cvs_constants(&lokappa0, &pownu0, &cterm);
     for (int r = 0; r < Lq; r++) {
         for (long long c = col0; c < col0 + ncols; c++) {
             int p = d_pro[c];
             float s = orc_init_score(q_tf + r, Lq, q_bkg, d_tf + c, N, d_bkg + p, P, prm->initshift);
             float ms = 0.0f;
+            int amb = 0;
+            const float cv = cvs ? orc_cvs_cell(prm, r, Lq, c, N, lokappa0, pownu0, cterm,
+                                                prm->cvs_ambiguous ? &amb : NULL)
+                                 : 0.0f;
+            if (prm->cvs_ambiguous) prm->cvs_ambiguous[(size_t)r * ld + (c - col0)] = (uint8_t)amb;
             if (prm->ssswgt > 0.0f) {
+                /* SS, plus the weighted CVS term in one addition
+                 * (CuBatchScoreMatrix_ssss_cvs2s.cu:252-270); the modular
+                 * score drops 0.5*CVSWGT */
                 float ss = orc_ss_score(q_ss + r, Lq, d_ss + c, N, ss_table, prm->ssswgt);
-                s = s + ss;
-                ms = ss;
+                if (cvs) {
+                    /* the reference kernel computes two columns per thread,
+                     * c and c+32 of each 64-column block of the chunk, and its
+                     * build fuses the addition for the first (one rounding)
+                     * but not for the second (the product rounded first) */
+                    ss = ((c >> 5) & 1) ? ss + cv * prm->cvswgt : fmaf(cv, prm->cvswgt, ss);
+                    s = s + ss;
+                    ms = ss - 0.5f * prm->cvswgt;
+                } else {
+                    s = s + ss;
+                    ms = ss;
+                }
+            } else if (cvs && cv != 0.0f) {
+                /* CVS alone (CuBatchScoreMatrix_cvs2s.cu:286-299), added
+                 * to a modular score that starts at zero */
+                s = s + cv * prm->cvswgt;
+                ms = ms + (cv - 0.5f) * prm->cvswgt;
             }
             if (prm->ddmswgt > 0.0f) {
                 float raw; int comp;
@@ -328,8 +413,10 @@ typedef struct {
 static void* orc_sm_thread(void* arg)
 {
     orc_sm_job* j = (orc_sm_job*)arg;
+    orc_score_params prm = *j->prm;   /* the flag output starts at this job's columns */
+    if (prm.cvs_ambiguous) prm.cvs_ambiguous += j->off;
     orc_score_matrix(j->Lq, j->q_tf, j->q_bkg, j->q_ss, j->q_dd, j->N, j->P, j->d_tf, j->d_bkg,
-                     j->d_pro, j->d_ss, j->d_dd, j->ss_table, j->prm, j->c0, j->nc,
+                     j->d_pro, j->d_ss, j->d_dd, j->ss_table, &prm, j->c0, j->nc,
                      j->scores + j->off, j->modscores + j->off, j->ld);
     return NULL;
 }

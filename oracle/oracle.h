@@ -38,7 +38,28 @@ typedef struct orc_score_params {
     float ddmswgt;    /* DDMSWGT */
     int   dstsegm;    /* DSTSEGM */
     float initshift;  /* 0.002 with MAPALN=1, 0.0003 otherwise */
+    /* context-vector (CVS) term, used when cvswgt > 0 */
+    float cvswgt;                 /* CVSWGT */
+    const float* q_cv;            /* query: [19][Lq] entries, [Lq] log priors, [Lq] squared norms */
+    const float* q_cvprior;
+    const float* q_cvnorm2;
+    const float* d_cv;            /* database: [19][N], [N], [N] */
+    const float* d_cvprior;
+    const float* d_cvnorm2;
+    const float* cvs_scores;      /* the CVS map: scores of keys (i - shift)/2, i < card */
+    int cvs_card, cvs_shift;
+    float cvs_key_first, cvs_key_last;
+    /* optional [Lq][ld] output: 1 where the map lookup of the cell would
+     * change within the error bound of the reference's fast logarithm */
+    uint8_t* cvs_ambiguous;
 } orc_score_params;
+
+/* constants of the context-vector score (src/libpro/srcpro/TCTXVECT.cpp:26-60) */
+void orc_cvs_constants(float* lokappa0, float* pownu0, float* cterm);
+
+/* CVS map value of a cell's log-odds score (GetScoreE1S1Step2Boundary,
+ * src/libmycu/cupro/SerializedCVS2Scores.cuh:377-410) */
+float orc_cvs_lookup(const orc_score_params* prm, float lo);
 
 /* natural logarithm restated from its series (see oracle.c) */
 float orc_logf(float x);

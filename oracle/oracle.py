@@ -61,6 +61,7 @@ def lib():
         L.orc_score_matrix.restype = None
         L.orc_score_matrix.argtypes = sm_args
         L.orc_score_matrix_mt.restype = None
+        L.orc_cvs_constants.restype = None
         L.orc_score_matrix_mt.argtypes = [ctypes.c_int] + sm_args
         L.orc_dp1_profile.restype = ctypes.c_float
         L.orc_dp1_profile.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong,
@@ -94,7 +95,31 @@ def ref_lib():
 
 class ScoreParams(ctypes.Structure):
     _fields_ = [("ssswgt", ctypes.c_float), ("ddmswgt", ctypes.c_float),
-                ("dstsegm", ctypes.c_int), ("initshift", ctypes.c_float)]
+                ("dstsegm", ctypes.c_int), ("initshift", ctypes.c_float),
+                ("cvswgt", ctypes.c_float),
+                ("q_cv", ctypes.c_void_p), ("q_cvprior", ctypes.c_void_p),
+                ("q_cvnorm2", ctypes.c_void_p),
+                ("d_cv", ctypes.c_void_p), ("d_cvprior", ctypes.c_void_p),
+                ("d_cvnorm2", ctypes.c_void_p),
+                ("cvs_scores", ctypes.c_void_p), ("cvs_card", ctypes.c_int),
+                ("cvs_shift", ctypes.c_int), ("cvs_key_first", ctypes.c_float),
+                ("cvs_key_last", ctypes.c_float), ("cvs_ambiguous", ctypes.c_void_p)]
+
+
+def load_cvs_map(path=None):
+    """The committed CVS map: dict(keys, scores, shift)."""
+    path = path or os.path.join(os.path.dirname(HERE), "tests", "golden", "cvs2s.npz")
+    z = np.load(path)
+    return {"keys": np.ascontiguousarray(z["keys"], np.float32),
+            "scores": np.ascontiguousarray(z["scores"], np.float32),
+            "shift": int(z["shift"])}
+
+
+def cvs_constants():
+    """(1/kappa0, -(nu0+2)/2, constant term) of the CVS score."""
+    a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+    lib().orc_cvs_constants(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    return a.value, b.value, c.value
 
 
 def logf(x: float) -> float:
@@ -116,8 +141,14 @@ def ddms_cell(qlist: np.ndarray, dlist: np.ndarray, dstsegm: int = 6, ddmswgt: f
 
 
 def score_matrix(query, db, ss_table, ssswgt=0.12, ddmswgt=0.2, dstsegm=6, initshift=0.002,
-                 col0=0, ncols=None, nthreads=1):
-    """(scores, modscores) [Lq][ncols] for query vs db columns [col0, col0+ncols)."""
+                 col0=0, ncols=None, nthreads=1, cvswgt=0.0, cvs_map=None, ambiguous=False):
+    """(scores, modscores) [Lq][ncols] for query vs db columns [col0, col0+ncols).
+
+    With cvswgt > 0 the context-vector term is added (both profile sets
+    must carry context vectors; the map defaults to the committed one);
+    with ambiguous=True a third array [Lq][ncols] (uint8) marks the cells
+    whose map lookup the reference's fast logarithm may move to a
+    neighbouring entry."""
     Lq = query.npositions
     N, P = db.npositions, db.nprofiles
     if ncols is None:
@@ -135,12 +166,31 @@ def score_matrix(query, db, ss_table, ssswgt=0.12, ddmswgt=0.2, dstsegm=6, inits
     sc = np.zeros((Lq, ncols), np.float32)
     ms = np.zeros((Lq, ncols), np.float32)
     prm = ScoreParams(ssswgt, ddmswgt, dstsegm, initshift)
+    keep = []
+    amb = np.zeros((Lq, ncols), np.uint8) if ambiguous else None
+    if cvswgt > 0.0:
+        if query.cv is None or db.cv is None:
+            raise ValueError("CVSWGT > 0 needs context vectors on both profile sets")
+        m = cvs_map or load_cvs_map()
+        arrs = [np.ascontiguousarray(x, np.float32) for x in
+                (query.cv, query.cvprior, query.cvnorm2, db.cv, db.cvprior, db.cvnorm2, m["scores"])]
+        keep += arrs
+        prm.cvswgt = float(cvswgt)
+        (prm.q_cv, prm.q_cvprior, prm.q_cvnorm2, prm.d_cv, prm.d_cvprior, prm.d_cvnorm2,
+         prm.cvs_scores) = [a.ctypes.data for a in arrs]
+        prm.cvs_card = len(m["scores"])
+        prm.cvs_shift = int(m["shift"])
+        prm.cvs_key_first = float(m["keys"][0])
+        prm.cvs_key_last = float(m["keys"][-1])
+        if amb is not None:
+            prm.cvs_ambiguous = amb.ctypes.data
     lib().orc_score_matrix_mt(int(nthreads), Lq, q_tf.ctypes.data, q_bkg.ctypes.data,
                               q_ss.ctypes.data, q_dd.ctypes.data, N, P, d_tf.ctypes.data,
                               d_bkg.ctypes.data, d_pro.ctypes.data, d_ss.ctypes.data,
                               d_dd.ctypes.data, T.ctypes.data, ctypes.byref(prm),
                               int(col0), int(ncols), sc.ctypes.data, ms.ctypes.data, int(ncols))
-    return sc, ms
+    del keep
+    return (sc, ms, amb) if ambiguous else (sc, ms)
 
 
 def dp1(query, db, scores, col0, p0, nprof, thld):

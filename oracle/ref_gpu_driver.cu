@@ -8,7 +8,7 @@
 // The launch sequence, grid shapes and device-heap arrangement restate the
 // reference's host code, not its kernels:
 //   score matrix   src/libmycu/cusco/CuBatchScoreMatrix.cu:122-404
-//                  (init, then SS, then DDMS; CVS and HDP off)
+//                  (init, then SS and/or CVS, then DDMS; HDP off)
 //   phase-1 DP     src/libmycu/cudp/CuBatchDP.cu:149-320 (host loop over
 //                  block diagonals) and FinalizeDP, :330-380
 //   statistics     src/libmycu/cuss/CuBatchSS.cu:60-160 (dynamic-parallel
@@ -31,6 +31,12 @@
 //                  triangle of the 30 x 30 table
 //   DMS table      SerializedDstMatchScoresCtor<float,2> has no entries
 //                  (SerializedDstMatchScores.cuh:632-645): cardinality 21.
+//   CVS map        serialized as SerializedCVS2ScoresCtor does
+//                  (src/libmycu/cupro/SerializedCVS2ScoresCtor.cuh:60-120) for
+//                  one level: level, cardinality, shift, scale, keys,
+//                  scores; attributes as CuDeviceMemory::CacheCVS2ScoresDevice
+//                  (CuDeviceMemory.cu:691-740), constants as _TCTXVECT
+//                  (src/libpro/srcpro/TCTXVECT.cpp:26-60).
 //
 // The database is passed as the chunk section (bdbC); the cached section is
 // empty. Profiles should come longest first, as in a reference database:
@@ -52,6 +58,9 @@
 #include "libmycu/cusco/CuBatchScoreMatrix_Init.cuh"
 #include "libmycu/cusco/CuBatchScoreMatrix_ssss.cuh"
 #include "libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh"
+#include "libmycu/cupro/SerializedCVS2ScoresAttr.h"
+#include "libmycu/cusco/CuBatchScoreMatrix_cvs2s.cuh"
+#include "libmycu/cusco/CuBatchScoreMatrix_ssss_cvs2s.cuh"
 #include "libmycu/cudp/CuBatchDP_com.h"
 #include "libmycu/cudp/CuBatchDP_init_btck.cuh"
 #include "libmycu/cudp/CuBatchDP_final.cuh"
@@ -172,6 +181,12 @@ typedef struct refgpu_job {
     // statistics and MAP, measured with events around each stage's launches
     int copy_matrices;
     float stage_ms[4];
+    // context-vector term: CVSWGT and the map (keys on the grid of halves,
+    // smoothed scores); the profiles' CV fields are in q/d
+    float cvswgt;
+    const float* cvskeys;
+    const float* cvsscores;
+    int cvscard;
 } refgpu_job;
 
 int refgpu_run(refgpu_job* J)
@@ -292,7 +307,47 @@ int refgpu_run(refgpu_job* J)
         float* modscores = (float*)(H + oMod);
         unsigned* glob = (unsigned*)(H + oGlob);
 
-        const bool modinuse = J->ssswgt > 0.0f;   // CVSWGT is 0 here
+        // CVS map and its attributes
+        SerializedCVS2ScoresAttr cvattr;
+        float* d_cvs = nullptr;
+        DevBuf cvsbuf;
+        if (J->cvswgt > 0.0f) {
+            const int card = J->cvscard;
+            int shift = 0;
+            while (shift < card && J->cvskeys[shift] < 0.0f) shift++;
+            std::vector<float> ser;
+            ser.push_back(1.0f);              // the one level
+            ser.push_back((float)card);
+            ser.push_back((float)shift);
+            ser.push_back(1.0f);              // scale
+            for (int i = 0; i < card; i++) ser.push_back(J->cvskeys[i]);
+            for (int i = 0; i < card; i++) ser.push_back(J->cvsscores[i]);
+            d_cvs = (float*)cvsbuf.alloc(up(ser.size() * sizeof(float), kAlign), "CVS map");
+            ck(cudaMemcpy(d_cvs, ser.data(), ser.size() * sizeof(float), cudaMemcpyHostToDevice),
+               "CVS map");
+            cvattr.ntotents_ = (int)ser.size();
+            cvattr.szalloc_ = (int)(ser.size() * sizeof(float));
+            cvattr.nenos_ = 1;
+            cvattr.ntbls_ = 1;
+            cvattr.card_ = card;
+            cvattr.shft_ = shift;
+            cvattr.key1first_ = J->cvskeys[0];
+            cvattr.value1first_ = J->cvsscores[0];
+            cvattr.key1last_ = J->cvskeys[card - 1];
+            cvattr.value1last_ = J->cvsscores[card - 1];
+            const int dim = 19;
+            const float kappa0 = 0.1f, nu0 = (float)dim;
+            const float pw = -0.5f * (nu0 + 2.f);
+            float ct = (0.5f * dim + pw) * (logf(kappa0) - logf(kappa0 + 2.f));
+            float sum = 0.0f;
+            for (int i = 1; i <= dim; i++) sum += logf(nu0 + 1.0f - i) - 0.69314718055994530942f;
+            ct += sum;
+            cvattr.CVS_loKAPPA0_ = 1.f / kappa0;
+            cvattr.CVS_PowerNU0_ = pw;
+            cvattr.CVS_CTERM_ = ct;
+        }
+
+        const bool modinuse = J->ssswgt > 0.0f || J->cvswgt > 0.0f;
         const uint nq = (uint)Lq, n1 = 0, nC = (uint)N, pad = (uint)dbxpad;
         Events ev;
         for (float& t : J->stage_ms) t = 0.0f;
@@ -306,10 +361,23 @@ int refgpu_run(refgpu_job* J)
         CalcSM_Init_SMEMUnroll2x<<<sblk, sthr>>>(nq, n1, nC, pad, 0, 0, 0,
                                                   CONSTINITSHIFT_MAPALN1, scores, NULL);
         ck_launch("init scores");
-        if (J->ssswgt > 0.0f) {
+        FtorRoundMAPALN1 ftor_mapaln1;
+        if (J->ssswgt > 0.0f && J->cvswgt > 0.0f) {
+            CalcSM_SSSS_CVS2S_SMEMUnroll2x<<<sblk, sthr, ssattr.szalloc_ + cvattr.szalloc_>>>(
+                d_ss, ssattr, J->ssswgt, d_cvs, cvattr, J->cvswgt, nq, n1, nC, pad, 0, 0, 0,
+                ftor_mapaln1, scores, modscores);
+            ck_launch("SS+CVS scores");
+        } else if (J->ssswgt > 0.0f) {
             CalcSM_SSSS_SMEMUnroll2x<<<sblk, sthr, ssattr.szalloc_>>>(
                 d_ss, ssattr, J->ssswgt, nq, n1, nC, pad, 0, 0, 0, scores, modscores);
             ck_launch("SS scores");
+        } else if (J->cvswgt > 0.0f) {
+            // the reference adds into modular scores it never initialised;
+            // start them at zero here
+            ck(cudaMemset(modscores, 0, Lq * dblen * sizeof(float)), "modscores");
+            CalcSM_CVS2S_SMEMUnroll2x<<<sblk, sthr, cvattr.szalloc_>>>(
+                d_cvs, cvattr, J->cvswgt, nq, n1, nC, pad, 0, 0, 0, ftor_mapaln1, scores, modscores);
+            ck_launch("CVS scores");
         }
         if (J->ddmswgt > 0.0f) {
             CalcSM_DDMS2S_SMEMUnroll2x_h2<DMS_STEP, DMS_LINEAR_INTERP_HALF, DMS_DSTBNDF>

@@ -16,6 +16,9 @@ tests and the benchmark need from it is committed:
                     returned by the reference's own CPU restatement
                     (cother-scores-optimizer/ddms.cxx:388-436, built by
                     oracle/Makefile into oracle/_ref/), rint(16 * top-3 sum)
+* cvs2s.npz      -- the context-vector score map of src/env/cvs2s as the
+                    reference's reader leaves it (keys, smoothed scores and
+                    the shift; see parse_cvs2s)
 """
 import os
 import sys
@@ -40,6 +43,92 @@ def parse_ssss(path):
             T[r, c] = v
             T[c, r] = v
     return T
+
+
+CVS_PLUS = np.float32(9999.0)   # the reader's value for a '+' score (CVS2Scores.cpp:39)
+
+
+def smooth_cvs_scores(keys, scos):
+    """CVS2Scores::SmoothScores (src/libpro/srcpro/CVS2Scores.cpp:366-460)
+    in float32: every score becomes the running average of 5 scores
+    ('+' entries skipped, the first two and the trailing ones take the
+    nearest full window), then keys missing from the 1/2 grid are inserted
+    with the previous smoothed score. Returns (keys, scores, shift), shift
+    being the number of negative keys."""
+    f32 = np.float32
+    n_ = len(scos)
+    plus = lambda v: CVS_PLUS <= v
+    smth = [f32(0)] * n_
+    rwin = [f32(0)] * 5
+    rsum, avg = f32(0), f32(0)
+    nv = rn = nn = 0
+    for n in range(n_):
+        sc = scos[n]
+        if nv < 2:
+            nn += 1
+        if not plus(sc):
+            if 5 <= rn:
+                rn = 0
+            rsum = f32(rsum - rwin[rn])
+            rwin[rn] = sc
+            rn += 1
+            rsum = f32(rsum + sc)
+            avg = f32(rsum / f32(5))
+            nv += 1
+        if 5 <= nv:
+            if not plus(sc):
+                if nv == 5:
+                    for p in range(nn):
+                        smth[p] = avg
+                smth[nn] = avg
+                nn += 1
+                while plus(scos[nn]) and nn < n:
+                    smth[nn] = avg
+                    nn += 1
+            if n_ == n + 1:
+                for p in range(nn, n_):
+                    smth[p] = avg
+    scos = list(scos)
+    sm = f32(0)
+    for n in range(n_ - 1, max(-1, n_ - 9999 - 1), -1):   # all: nSLAST = 9999
+        sm = smth[n]
+        scos[n] = sm
+    keys = list(keys)
+    incr = f32(0.5)
+    pkk = f32(0)
+    n = 0
+    while n < len(keys):
+        kk, sc = keys[n], scos[n]
+        if n and kk <= pkk:
+            raise ValueError("CVS keys are not sorted")
+        if n and incr < f32(kk - pkk):
+            pkk = f32(pkk + incr)
+            keys.insert(n, pkk)
+            scos.insert(n, sm)
+            smth.insert(n, sm)
+            n += 1
+            continue
+        pkk = kk
+        sm = smth[n]
+        if plus(sc):
+            scos[n] = sm
+        n += 1
+    shift = next((i for i, k in enumerate(keys) if f32(0) <= k), len(keys))
+    return np.array(keys, np.float32), np.array(scos, np.float32), shift
+
+
+def parse_cvs2s(path):
+    """The single table of src/env/cvs2s (one level of effective sequence
+    numbers, read by CVS2Scores::ReadScoresHelper,
+    src/libpro/srcpro/CVS2Scores.cpp:206-357), smoothed as the reader does."""
+    lines = open(path).read().splitlines()
+    i = next(k for k, ln in enumerate(lines) if ln.strip().startswith("Cardinality"))
+    card = int(lines[i].split("=")[1])
+    rest = [ln for ln in lines[i + 1:] if ln.strip() and not ln.lstrip().startswith("#")]
+    keys = [np.float32(v) for v in rest[0].split()[:card]]
+    scos = [CVS_PLUS if v == "+" else np.float32(v) for v in rest[1].split()[:card]]
+    assert len(keys) == card and len(scos) == card
+    return smooth_cvs_scores(keys, scos)
 
 
 def parse_nn_weights(path):
@@ -96,6 +185,9 @@ if __name__ == "__main__":
     par = parse_cother_par(os.path.join(REF, "src/env/cother.par"))
     json.dump({k: par[k] for k in ("UNGAPPED", "GAPPED_A_1")},
               open(os.path.join(HERE, "cother_par.json"), "w"), indent=1)
+    ck, cs, cshift = parse_cvs2s(os.path.join(REF, "src/env/cvs2s"))
+    np.savez(os.path.join(HERE, "cvs2s.npz"), keys=ck, scores=cs, shift=np.int32(cshift))
+    print("cvs2s", len(ck), "keys", float(ck[0]), "..", float(ck[-1]), "shift", cshift)
     qa, da, ref = ddms_vectors()
     np.savez_compressed(os.path.join(HERE, "ddms_ref.npz"), qlists=qa, dlists=da, ref=ref)
     print("ssss", T.shape, "ddms pairs", len(ref), "scored", int((ref != -777).sum()))

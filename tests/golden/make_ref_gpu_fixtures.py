@@ -12,7 +12,8 @@ does the same and checks ``input_digest`` first). The reference tree is not
 read at run time: only the prebuilt library and the committed fixtures
 (ssss.npy, nn_weights.npy, cother_par.json) are.
 
-Usage (on a machine with a B200):  python tests/golden/make_ref_gpu_fixtures.py [outdir]
+Usage (on a machine with a B200):
+    python tests/golden/make_ref_gpu_fixtures.py [outdir [case,case,...]]
 """
 from __future__ import annotations
 
@@ -47,6 +48,12 @@ CASES = {
                      full=False),
     "noss": dict(ssswgt=0.0, ddmswgt=0.2, dstsegm=6, minpp=0.28, ssemodel=2, xuninf=1,
                  full=True),
+    # the context-vector term at the reference's default weight, with and
+    # without the SS term (inputs with context vectors)
+    "cvs": dict(ssswgt=0.12, cvswgt=0.15, ddmswgt=0.2, dstsegm=6, minpp=0.28, ssemodel=2,
+                xuninf=1, full=True, inputs="q64cv"),
+    "cvs_only": dict(ssswgt=0.0, cvswgt=0.15, ddmswgt=0.2, dstsegm=6, minpp=0.28, ssemodel=2,
+                     xuninf=1, full=True, inputs="q64cv"),
 }
 # every profile passes phase 1, so that each one's phase-1 record and
 # statistics are pinned; MAP realigns the pairs with log E <= LOGE_THLD
@@ -68,6 +75,7 @@ def search_space(q, db) -> float:
 INPUTS = {
     "q64": dict(qlen=64, nprof=16, median=90, lo=30, hi=220, seed=611),
     "q77": dict(qlen=77, nprof=12, median=120, lo=30, hi=300, seed=711),
+    "q64cv": dict(qlen=64, nprof=16, median=90, lo=30, hi=220, seed=611, cv=True),
 }
 
 
@@ -79,6 +87,9 @@ def case_inputs(name: str = "q64"):
     lens = synth.lognormal_lengths(c["nprof"], c["median"], c["lo"], c["hi"], seed=c["seed"] + 1)
     lens = np.sort(np.asarray(lens))[::-1].copy()
     db = synth.make_profiles(lens, seed=c["seed"] + 2, predicted=False, nthreads=1)
+    if c.get("cv"):
+        synth.add_context_vectors(q, c["seed"] + 10)
+        synth.add_context_vectors(db, c["seed"] + 11)
     synth.plant_homologs(q, db, 2.0 / c["nprof"], seed=c["seed"] + 3)
     return q, db
 
@@ -89,6 +100,9 @@ def input_digest(q, db) -> str:
         for a in (ps.lens, ps.bkg, ps.eno, ps.trn, ps.tf, ps.dd, ps.ss, ps.addrpro, ps.aa,
                   ps.ssstate):
             h.update(np.ascontiguousarray(a).tobytes())
+        if ps.cv is not None:
+            for a in (ps.cv, ps.cvprior, ps.cvnorm2):
+                h.update(np.ascontiguousarray(a).tobytes())
     return h.hexdigest()
 
 
@@ -109,6 +123,8 @@ class Job(ctypes.Structure):
         ("alns", ctypes.c_void_p), ("alns_cap", ctypes.c_size_t),
         ("globvars", ctypes.c_uint * 4), ("dblen", ctypes.c_int), ("dbalnlen2", ctypes.c_size_t),
         ("copy_matrices", ctypes.c_int), ("stage_ms", ctypes.c_float * 4),
+        ("cvswgt", ctypes.c_float), ("cvskeys", ctypes.c_void_p), ("cvsscores", ctypes.c_void_p),
+        ("cvscard", ctypes.c_int),
     ]
 
 
@@ -139,6 +155,11 @@ def run_case(L, q, db, opts):
     j.reflambda, j.refK = par["UNGAPPED"]["Lambda"], par["UNGAPPED"]["K"]
     j.explambda, j.expK = par["GAPPED_A_1"]["Lambda"], par["GAPPED_A_1"]["K"]
     j.dstsegm, j.ssemodel, j.xuninf = opts["dstsegm"], opts["ssemodel"], opts["xuninf"]
+    cvs = np.load(os.path.join(HERE, "cvs2s.npz"))
+    cvkeys = np.ascontiguousarray(cvs["keys"], np.float32)
+    cvscores = np.ascontiguousarray(cvs["scores"], np.float32)
+    j.cvswgt = opts.get("cvswgt", 0.0)
+    j.cvskeys, j.cvsscores, j.cvscard = cvkeys.ctypes.data, cvscores.ctypes.data, len(cvkeys)
     sc = np.zeros((Lq, dblen), np.float32)
     ms = np.zeros((Lq, dblen), np.float32)
     bt = np.zeros((Lq, dblen), np.uint8)
@@ -166,11 +187,13 @@ def run_case(L, q, db, opts):
     return out
 
 
-def main(outdir: str) -> None:
+def main(outdir: str, only=None) -> None:
     L = ctypes.CDLL(LIB)
     L.refgpu_error.restype = ctypes.c_char_p
     os.makedirs(outdir, exist_ok=True)
     for name, opts in CASES.items():
+        if only and name not in only:
+            continue
         q, db = case_inputs(opts.get("inputs", "q64"))
         out = run_case(L, q, db, opts)
         path = os.path.join(outdir, f"ref_gpu_{name}.npz")
@@ -179,4 +202,6 @@ def main(outdir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    # usage: make_ref_gpu_fixtures.py [outdir [case,case,...]]
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE,
+         sys.argv[2].split(",") if len(sys.argv) > 2 else None)

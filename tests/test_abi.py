@@ -35,10 +35,19 @@ def test_defaults_and_errors_without_gpu():
     # creating a context with an invalid option must fail with a message,
     # never abort the process
     bad = cb.Options.defaults()
-    bad.cvswgt = 0.15
+    bad.cvswgt = 1.5             # CVSWGT is in [0, 1) (MOptions.cpp)
     h = ctypes.c_void_p()
     import numpy as np
     t = np.zeros((30, 30), np.float32)
     rc = lib.cbp_create(0, ctypes.byref(bad), t.ctypes.data, 0, ctypes.byref(h))
     assert rc != 0
     assert b"CVSWGT" in lib.cbp_last_error()
+
+
+def test_slab_bytes_is_host_only():
+    """The slab planner's charge needs no device: linear in the slab's
+    positions, growing with the query length."""
+    import cother_b200 as cb
+    a, b = cb.slab_bytes(400, 1000), cb.slab_bytes(400, 2000)
+    assert 0 < a < b and b - a == cb.slab_bytes(400, 1000) - cb.slab_bytes(400, 0)
+    assert cb.slab_bytes(800, 1000) > a

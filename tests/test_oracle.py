@@ -1,6 +1,7 @@
 """CPU tests of the oracle: pinned against the reference's own CPU code and
 golden vectors (no GPU)."""
 import os
+import sys
 
 import numpy as np
 import pytest
@@ -101,3 +102,32 @@ def test_library_nn_weights_equal_fixture():
     ref = np.load(os.path.join(GOLDEN, "nn_weights.npy"))
     assert vals.shape == ref.shape
     assert np.array_equal(vals, ref)
+
+
+def test_cvs_map_smoothing_and_fixture():
+    """The CVS map reader's smoothing (CVS2Scores::SmoothScores): 5-point
+    running means, the first entries taking the first full window and the
+    trailing ones (and '+' entries) the last; and the committed map."""
+    sys.path.insert(0, GOLDEN)
+    import make_fixtures as mf
+    f = np.float32
+    k = [f(x) for x in (-1.0, -0.5, 0.0, 0.5, 1.0, 1.5, 2.0)]
+    keys, sc, shift = mf.smooth_cvs_scores(k, [f(x) for x in (1, 2, 3, 4, 5, 6, 7)])
+    assert shift == 2 and np.array_equal(sc, np.array([3, 3, 3, 4, 5, 5, 5], np.float32))
+    _, sc, _ = mf.smooth_cvs_scores(k, [f(x) for x in (1, 2, 3, 4, 5, 6)] + [mf.CVS_PLUS])
+    assert np.array_equal(sc, np.array([3, 3, 3, 4, 4, 4, 4], np.float32))
+    z = np.load(os.path.join(GOLDEN, "cvs2s.npz"))
+    keys, scores, shift = z["keys"], z["scores"], int(z["shift"])
+    assert len(keys) == len(scores) == 93 and shift == 5
+    assert np.array_equal(keys, (np.arange(93, dtype=np.float32) - 5) * np.float32(0.5))
+    assert np.all(np.isfinite(scores)) and scores[0] < 0 < scores[-1]
+
+
+def test_cvs_constants(oracle_lib):
+    """1/kappa0, -(nu0+2)/2 and the constant term of the CVS log-odds."""
+    lk, pw, ct = oracle_lib.cvs_constants()
+    assert lk == np.float32(10.0) and pw == np.float32(-10.5)
+    import math
+    exact = (9.5 - 10.5) * (math.log(0.1) - math.log(2.1)) + sum(
+        math.log(20 - i) - math.log(2) for i in range(1, 20))
+    assert abs(ct - exact) < 1e-4

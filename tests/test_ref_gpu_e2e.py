@@ -13,7 +13,8 @@ the same query, database and options on a B200
 
 The two paths differ only in the profile-profile term's log (the
 reference's __logf intrinsic, a series restatement here), a few ulps per
-cell.
+cell; the modular scores, which do not contain that term, are compared bit
+for bit where the fixture holds them (the CVS term included).
 """
 import json
 import os
@@ -40,7 +41,11 @@ def test_search_matches_reference_kernels(case, ss_table):
     o = cb.Options.defaults()
     o.ssswgt, o.ddmswgt, o.dstsegm = opts["ssswgt"], opts["ddmswgt"], opts["dstsegm"]
     o.minpp, o.ssemodel, o.x_uninf = opts["minpp"], opts["ssemodel"], opts["xuninf"]
+    o.cvswgt = opts.get("cvswgt", 0.0)
     with cb.BatchProcessing(ss_table, o) as bp:
+        if o.cvswgt > 0:
+            m = np.load(os.path.join(GOLDEN, "cvs2s.npz"))
+            bp.set_cvs2s_map(m["keys"], m["scores"])
         bp.set_db_details(db.npositions, db.nprofiles)
         bp.set_score_threshold(float(F["scorethld"]))
         bp.set_logE_threshold(float(F["logevthld"]))
@@ -49,6 +54,11 @@ def test_search_matches_reference_kernels(case, ss_table):
         assert bp.search_space()[0] == int(F["searchspace"])
         recs = cb.records_table(bp.hit_records())
         alns = bp.alignments(q.npositions)
+        if "modscores" in F:
+            # modular scores (SS, CVS and DDMS terms; the CVS term with the
+            # same __logf intrinsic) bit for bit
+            _, ms, _ = bp.read_score_matrix(q.npositions, db.npositions)
+            assert np.array_equal(ms, F["modscores"][:, :db.npositions])
 
     st, fin, rows = F["stats"], F["final"], F["alns"]
     ref_org = st[:, 1].view(np.uint32).astype(np.int64)

@@ -11,6 +11,10 @@ def _run(q, db, ss_table, max_slab=0, **opt):
     for k, v in opt.items():
         setattr(o, k, v)
     with cb.BatchProcessing(ss_table, o) as bp:
+        if o.cvswgt > 0:
+            from oracle import oracle as O
+            m = O.load_cvs_map()
+            bp.set_cvs2s_map(m["keys"], m["scores"])
         if max_slab:
             bp.set_max_slab_positions(max_slab)
         bp.transfer_cpm_data(db)
@@ -69,6 +73,40 @@ def test_score_matrix_options(oracle_lib, ss_table):
         osc, oms = oracle_lib.score_matrix(q, db, ss_table, **orc)
         assert np.array_equal(sc, osc), opt
         assert np.array_equal(ms, oms), opt
+
+
+@pytest.mark.parametrize("ssswgt", [0.12, 0.0])
+def test_score_matrix_context_vectors(oracle_lib, ss_table, ssswgt):
+    """The CVS term (CVSWGT 0.15, with and without SS) against the oracle:
+    bit for bit except where the oracle flags the map lookup as within the
+    error bound of the __logf intrinsic of a map edge; those cells differ by
+    at most one map step."""
+    from cother_b200 import synth
+    q, db = synth.make_workload("q200_db1k", seed=4, ndb=40, context_vectors=True)
+    sc, ms, _ = _run(q, db, ss_table, ssswgt=ssswgt, cvswgt=0.15)
+    osc, oms, amb = oracle_lib.score_matrix(q, db, ss_table, ssswgt=ssswgt, cvswgt=0.15,
+                                            ambiguous=True, nthreads=16)
+    amb = amb.astype(bool)
+    step = float(np.max(np.abs(np.diff(oracle_lib.load_cvs_map()["scores"])))) * 0.15 + 1e-6
+    assert amb.mean() < 1e-3
+    assert np.array_equal(sc[~amb], osc[~amb]) and np.array_equal(ms[~amb], oms[~amb])
+    assert np.all(np.abs(sc - osc)[amb] <= step) and np.all(np.abs(ms - oms)[amb] <= step)
+    # the term is there: it moves the scores
+    plain = oracle_lib.score_matrix(q, db, ss_table, ssswgt=ssswgt, nthreads=16)[0]
+    assert np.abs(osc - plain).mean() > 1e-3
+
+
+def test_context_vectors_need_map_and_fields(ss_table):
+    import cother_b200 as cb
+    from cother_b200 import synth
+    q = synth.make_profiles([20], 51, True)
+    db = synth.make_profiles([30, 40], 52, False)
+    o = cb.Options.defaults()
+    o.cvswgt = 0.15
+    with cb.BatchProcessing(ss_table, o) as bp:
+        bp.transfer_cpm_data(synth.add_context_vectors(db, 53))
+        with pytest.raises(cb.CbpError, match="context-vector map"):
+            bp.process_score_matrix(synth.add_context_vectors(q, 54))
 
 
 def test_bad_inputs_fail_loudly(ss_table):
