@@ -74,6 +74,7 @@ def load_library(path: str | None = None):
         "cbp_set_score_threshold": (i32, [vp, f32]),
         "cbp_set_logE_threshold": (i32, [vp, f32]),
         "cbp_set_cvs2s_map": (i32, [vp, vp, vp, sz]),
+        "cbp_read_statistics": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_transfer_chunk": (i32, [vp, vp, vp, vp]),
         "cbp_process": (i32, [vp, i32, sz, vp, vp]),
         "cbp_wait_idle": (i32, [vp]),
@@ -255,6 +256,17 @@ class BatchProcessing:
                                                      ctypes.byref(ncols), ctypes.byref(first)))
         n = ncols.value
         return sc[:, :n], ms[:, :n], first.value
+
+    def read_statistics(self) -> np.ndarray:
+        """Hit records [npass][CBP_REC_FLOATS] of the last slab as the
+        statistics stage leaves them (before the phase-2 finalizer)."""
+        L = load_library()
+        n = ctypes.c_size_t()
+        _check(L.cbp_read_statistics(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, REC_FLOATS), np.float32)
+        if n.value:
+            _check(L.cbp_read_statistics(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
 
     def read_phase1(self):
         """Phase-1 records of the last slab: dict of arrays (score, psts,

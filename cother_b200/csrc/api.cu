@@ -182,7 +182,7 @@ struct cbp_context {
     float cvs_key_first = 0.f, cvs_key_last = 0.f;
     // working buffers
     DevBuf scores, modscores, btck, bandbuf, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
-    DevBuf hitrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf;
+    DevBuf hitrecs, statrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf;
     std::vector<char> h_alns[5];
     long long base_len = 0, base_npass = 0;   // running phase-2 offsets over slabs
     long long last_npos2 = 0;
@@ -528,7 +528,7 @@ int cbp_destroy(cbp_context* c)
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax, &c->dpcoords,
                       &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
                       &c->cs2, &c->fb2, &c->sg2, &c->bt2, &c->strip2, &c->maperr, &c->alnbuf,
-                      &c->cvsmap})
+                      &c->cvsmap, &c->statrecs})
         b->release();
     c->sstab.release();
     c->dmstab.release();
@@ -722,6 +722,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 a.cvs_key_first = c->cvs_key_first;
                 a.cvs_key_last = c->cvs_key_last;
                 cvs_constants(&a.cvs_lokappa0, &a.cvs_pownu0, &a.cvs_cterm);
+                a.cvs_int_priors = !c->opt.mapaln;
             }
             a.sstab = c->sstab.as<float>();
             a.dmstab = c->dmstab.as<float>();
@@ -822,6 +823,11 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 CBP_CUDA(cudaEventRecord(c->ev[4], c->stream));
                 launch_stats(st, npass, c->stream);
                 CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
+                // the records as the statistics leave them (cbp_read_statistics)
+                c->statrecs.reserve((size_t)npass * kRecFloats * sizeof(float));
+                CBP_CUDA(cudaMemcpyAsync(c->statrecs.p, c->hitrecs.p,
+                                         (size_t)npass * kRecFloats * sizeof(float),
+                                         cudaMemcpyDeviceToDevice, c->stream));
                 c->launches += 1;
                 c->stage_launches[3] += 1;
 
@@ -834,6 +840,29 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 const long long nd = map_diag_rows(npos2);
                 const size_t nb = (size_t)map_bands(Lq);
                 const long long alnstride = align_up(npos2 + (long long)npass * Lq, 32);
+                c->alnbuf.reserve(5 * (size_t)alnstride);
+                MapArgs mp;
+                mp.scores = a.scores;
+                mp.modscores = a.modscores;
+                mp.ld = a.ld;
+                mp.Lq = Lq;
+                mp.col0 = s.col0;
+                mp.p0 = s.p0;
+                mp.db = c->db->view;
+                mp.qtrn = c->query.view.trn;
+                mp.qaa = c->query.view.aa;
+                mp.qsss = c->query.view.sss;
+                mp.printsss = c->opt.ssswgt > 0.0f;
+                mp.modscores_inuse = (c->opt.ssswgt > 0.0f || c->opt.cvswgt > 0.0f) ? 1 : 0;
+                mp.minpp = c->opt.minpp;
+                mp.logevthld = c->logE_thld;
+                mp.npass = npass;
+                mp.pass_idx = c->passidx.as<int>();
+                mp.pass_dst = c->passdst.as<long long>();
+                mp.recs = c->hitrecs.as<float>();
+                mp.alns = c->alnbuf.as<char>();
+                mp.alnstride = alnstride;
+                CBP_CUDA(cudaMemsetAsync(c->alnbuf.p, 0, 5 * (size_t)alnstride, c->stream));
                 if (c->opt.mapaln) {
                     c->cs2.reserve(nb * nd * 32 * sizeof(float));
                     c->fb2.reserve(nb * nd * 32 * sizeof(float));
@@ -841,26 +870,6 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                     c->bt2.reserve(nb * nd * sizeof(unsigned long long));
                     c->strip2.reserve((size_t)map_strip_floats(npos2) * sizeof(float));
                     c->maperr.reserve(sizeof(int));
-                    c->alnbuf.reserve(5 * (size_t)alnstride);
-                    MapArgs mp;
-                    mp.scores = a.scores;
-                    mp.modscores = a.modscores;
-                    mp.ld = a.ld;
-                    mp.Lq = Lq;
-                    mp.col0 = s.col0;
-                    mp.p0 = s.p0;
-                    mp.db = c->db->view;
-                    mp.qtrn = c->query.view.trn;
-                    mp.qaa = c->query.view.aa;
-                    mp.qsss = c->query.view.sss;
-                    mp.printsss = c->opt.ssswgt > 0.0f;
-                    mp.modscores_inuse = (c->opt.ssswgt > 0.0f || c->opt.cvswgt > 0.0f) ? 1 : 0;
-                    mp.minpp = c->opt.minpp;
-                    mp.logevthld = c->logE_thld;
-                    mp.npass = npass;
-                    mp.pass_idx = c->passidx.as<int>();
-                    mp.pass_dst = c->passdst.as<long long>();
-                    mp.recs = c->hitrecs.as<float>();
                     mp.nd = nd;
                     mp.cs = c->cs2.as<float>();
                     mp.fb = c->fb2.as<float>();
@@ -868,9 +877,6 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                     mp.bt = c->bt2.as<unsigned long long>();
                     mp.strip = c->strip2.as<float>();
                     mp.err = c->maperr.as<int>();
-                    mp.alns = c->alnbuf.as<char>();
-                    mp.alnstride = alnstride;
-                    CBP_CUDA(cudaMemsetAsync(c->alnbuf.p, 0, 5 * (size_t)alnstride, c->stream));
                     CBP_CUDA(cudaMemsetAsync(c->maperr.p, 0, sizeof(int), c->stream));
                     CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
                     launch_map(mp, c->stream);
@@ -879,8 +885,17 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                                              cudaMemcpyDeviceToHost, c->stream));
                     c->launches += 2;
                     c->stage_launches[4] += 2;
-                    c->last_npos2 = npos2;
+                } else {
+                    // MAPALN=0: the phase-1 alignments themselves
+                    // (CuBatchDP::FinalizeALNDynProgDevice)
+                    CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
+                    launch_aln_final(mp, c->btck.as<uint8_t>(), c->dpmax.as<float>(),
+                                     c->dpcoords.as<uint32_t>(), c->stream);
+                    CBP_CUDA(cudaEventRecord(c->ev[7], c->stream));
+                    c->launches += 1;
+                    c->stage_launches[4] += 1;
                 }
+                c->last_npos2 = npos2;
                 const size_t off = c->h_recs.size();
                 c->h_recs.resize(off + (size_t)npass * kRecFloats);
                 CBP_CUDA(cudaMemcpyAsync(c->h_recs.data() + off, c->hitrecs.p,
@@ -892,10 +907,9 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 const long long slablen = npos2 + (long long)npass * Lq;
                 for (int row = 0; row < 5; row++) {
                     c->h_alns[row].resize((size_t)(shift + slablen), 0);
-                    if (c->opt.mapaln)
-                        CBP_CUDA(cudaMemcpyAsync(c->h_alns[row].data() + shift,
-                                                 c->alnbuf.as<char>() + (size_t)row * alnstride,
-                                                 (size_t)slablen, cudaMemcpyDeviceToHost, c->stream));
+                    CBP_CUDA(cudaMemcpyAsync(c->h_alns[row].data() + shift,
+                                             c->alnbuf.as<char>() + (size_t)row * alnstride,
+                                             (size_t)slablen, cudaMemcpyDeviceToHost, c->stream));
                 }
                 CBP_CUDA(cudaStreamSynchronize(c->stream));
                 if (c->opt.mapaln && c->h_maperr)
@@ -903,10 +917,8 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                                               "timed out");
                 CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
                 c->stage_ms[3] += ms;
-                if (c->opt.mapaln) {
-                    CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]));
-                    c->stage_ms[4] += ms;
-                }
+                CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]));
+                c->stage_ms[4] += ms;
                 // phase-2 offsets of this slab's pairs become offsets in the
                 // whole result
                 for (size_t i = off; i < c->h_recs.size(); i += kRecFloats) {
@@ -969,6 +981,21 @@ int cbp_read_phase1(cbp_context* c, float* score, float* psts, uint32_t* beg, ui
         if (pass_list && c->last_npass > 0)
             CBP_CUDA(cudaMemcpy(pass_list, c->passidx.p, (size_t)c->last_npass * sizeof(int),
                                 cudaMemcpyDeviceToHost));
+    });
+}
+
+int cbp_read_statistics(cbp_context* c, float* recs, size_t nmax, size_t* npass)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!c->last_Lq) throw Error(CBP_ERR_STATE, "no processed query");
+        const size_t n = (size_t)c->last_npass;
+        if (npass) *npass = n;
+        if (!recs || n == 0) return;
+        if (nmax < n) throw Error(CBP_ERR_ARG, "output array too small");
+        CBP_CUDA(cudaStreamSynchronize(c->stream));
+        CBP_CUDA(cudaMemcpy(recs, c->statrecs.p, n * kRecFloats * sizeof(float),
+                            cudaMemcpyDeviceToHost));
     });
 }
 

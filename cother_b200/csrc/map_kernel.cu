@@ -828,7 +828,106 @@ map_kernel(const MapArgs a, int nb)
     }
 }
 
+// ---------------------------------------------------------------------------
+// MAPALN=0 (FinalizeDP_ALN, src/libmycu/cudp/CuBatchDP_aln_final.cu:40-430):
+// one warp per pair of the pass list within the E-value threshold; lane 0
+// walks the phase-1 backtrack codes from the phase-1 maximum (the origin
+// when that maximum is not positive) and the warp writes the strings in
+// windows of 32, right-aligned in the pair's slot, as the MAP finalizer.
+constexpr int kAlnWarps = 4;
+
+__global__ void __launch_bounds__(32 * kAlnWarps)
+aln_final_kernel(const MapArgs a, const uint8_t* __restrict__ btck1, const float* __restrict__ maxsc1,
+                 const uint32_t* __restrict__ maxcoords1)
+{
+    __shared__ char s_win[kAlnWarps][5][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int k = blockIdx.x * kAlnWarps + w;
+    if (k >= a.npass) return;   // whole warp
+    float* rec = a.recs + (long long)k * kRecFloats;
+    if (a.logevthld < rec[rEvalue]) {
+        if (lane == 0) rec[rEpA] = __int_as_float(0);
+        return;
+    }
+    const int pl = a.pass_idx[k];
+    const int p = a.p0 + pl;
+    const int Lq = a.Lq, Ld = a.db.plen[p];
+    const long long pstart = a.db.pstart[p];
+    const long long colb = pstart - a.col0;
+    const uint8_t* __restrict__ B = btck1 + colb;
+    const float* __restrict__ S = a.scores + colb;
+    const uint32_t xx = (0.0f < maxsc1[pl]) ? maxcoords1[pl] : 0u;
+    int x = (int)(xx >> 16), y = (int)(xx & 0xffff);
+    const long long term = a.pass_dst[k] + (long long)k * Lq + Ld + Lq - 1;
+    if (lane < 5) a.alns[(long long)lane * a.alnstride + term] = 0;
+    const int8_t* qaa = a.qaa;
+    const int8_t* daa = a.db.aa + pstart;
+    const int8_t* qss = a.qsss;
+    const int8_t* dss = a.db.sss + pstart;
+    const bool prss = a.printsss;
+    char (*win)[32] = s_win[w];
+    int idts = 0, psts = 0, gaps = 0, alnlen = 0, b = 3;
+    while (b != 0) {
+        int n = 0;
+        if (lane == 0) {
+            for (; n < 32;) {
+                if (x < 0 || y < 0) { b = 0; break; }
+                b = B[(long long)y * a.ld + x];
+                if (b == 0) break;
+                char cq, cm, ct, sq = ' ', st = ' ';
+                if (b == 2) {
+                    gaps++;
+                    cq = (char)qaa[y]; ct = '-'; cm = ' ';
+                    if (prss) sq = (char)qss[y];
+                    y--;
+                } else if (b == 1) {
+                    gaps++;
+                    cq = '-'; ct = (char)daa[x]; cm = ' ';
+                    if (prss) st = (char)dss[x];
+                    x--;
+                } else {
+                    cq = (char)qaa[y]; ct = (char)daa[x];
+                    if (prss) { sq = (char)qss[y]; st = (char)dss[x]; }
+                    if (cq == ct) { cm = cq; idts++; }
+                    else if (S[(long long)y * a.ld + x] > 0.0f) { cm = '+'; psts++; }
+                    else cm = ' ';
+                    x--; y--;
+                }
+                win[0][n] = cq; win[1][n] = cm; win[2][n] = ct; win[3][n] = sq; win[4][n] = st;
+                n++;
+            }
+        }
+        __syncwarp();
+        b = __shfl_sync(kFull, b, 0);
+        n = __shfl_sync(kFull, n, 0);
+        if (lane < n) {
+            const long long pos = term - alnlen - 1 - lane;
+#pragma unroll
+            for (int row = 0; row < 5; row++) a.alns[(long long)row * a.alnstride + pos] = win[row][lane];
+        }
+        alnlen += n;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        rec[rPstvs] = (float)psts;
+        rec[rBegCoords] = __int_as_float((int)(((uint32_t)(x + 1) << 16) | (uint32_t)(y + 1)));
+        rec[rEndCoords] = __int_as_float((int)xx);
+        rec[rIdnts] = (float)idts;
+        rec[rNGaps] = (float)gaps;
+        rec[rEpA] = __int_as_float(alnlen);
+    }
+}
+
 }  // namespace
+
+void launch_aln_final(const MapArgs& a, const uint8_t* btck1, const float* maxsc1,
+                      const uint32_t* maxcoords1, cudaStream_t stream)
+{
+    if (a.npass <= 0) return;
+    aln_final_kernel<<<(unsigned)ceil_div(a.npass, kAlnWarps), 32 * kAlnWarps, 0, stream>>>(
+        a, btck1, maxsc1, maxcoords1);
+    CBP_CHECK_LAUNCH();
+}
 
 void launch_map(const MapArgs& a, cudaStream_t stream)
 {

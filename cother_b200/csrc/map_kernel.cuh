@@ -57,4 +57,12 @@ inline long long map_strip_floats(long long npos2)
 // zeroes sg and bt, then realigns every pair of the pass list
 void launch_map(const MapArgs& a, cudaStream_t stream);
 
+// MAPALN=0: alignment rows and counts of the pass list's pairs from their
+// phase-1 backtrack codes ([Lq][ld] of the slab), starting at the phase-1
+// maximum (maxsc1/maxcoords1 per slab profile). Uses the slab, query,
+// pass-list, record and alignment-row fields of `a`, not the phase-2
+// buffers.
+void launch_aln_final(const MapArgs& a, const uint8_t* btck1, const float* maxsc1,
+                      const uint32_t* maxcoords1, cudaStream_t stream);
+
 }  // namespace cbp

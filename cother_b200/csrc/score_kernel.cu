@@ -202,6 +202,10 @@ __device__ __forceinline__ float cvs_cell(const ScoreArgs& a, const float* __res
     const float qa = qnorm2 + 1.0f + a.cvs_lokappa0;
     const float da = dnorm2 + 1.0f + a.cvs_lokappa0;
     const float det = __fmaf_rn(qa, da, -(dot * dot));
+    if (a.cvs_int_priors) {   // FtorRoundMAPALN0 (CuBatchScoreMatrix_cvs2s.cuh:38-41)
+        qprior = (float)(int)qprior;
+        dprior = (float)(int)dprior;
+    }
     const float lo = __fmaf_rn(a.cvs_pownu0, __logf(det), a.cvs_cterm) - qprior - dprior;
     if (!(a.cvs_key_first < lo)) return __ldg(a.cvs_scores);
     if (a.cvs_key_last <= lo) return __ldg(a.cvs_scores + a.cvs_card - 1);

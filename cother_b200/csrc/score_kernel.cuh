@@ -22,6 +22,7 @@ struct ScoreArgs {
     int cvs_card = 0, cvs_shift = 0;
     float cvs_key_first = 0.f, cvs_key_last = 0.f;
     float cvs_lokappa0 = 0.f, cvs_pownu0 = 0.f, cvs_cterm = 0.f;
+    bool cvs_int_priors = false;    // MAPALN=0: log priors truncated to integers
     const float* sstab = nullptr;   // [30][30]
     const float* dmstab = nullptr;  // [22][22]
     float* scores = nullptr;        // [Lq][ld]

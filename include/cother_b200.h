@@ -188,6 +188,14 @@ int cbp_read_phase1(cbp_context* ctx, float* score, float* psts, uint32_t* beg,
                     uint32_t* end, int* passed, size_t nmax, size_t* nprof,
                     int* pass_list, size_t* npass);
 
+/* The hit records of the last slab's passed pairs as the statistics stage
+ * leaves them (CBP_REC_FLOATS floats each, pass-list order), before the
+ * phase-2 finalizer overwrites the positives, coordinates, counts and the
+ * per-pair log E-value slot (the reference's dp2alndatbuffers between
+ * CalculateAlnStatisticsDevice and the MAP stage,
+ * src/libmycu/cupro/CuBatchProcessing.cu:430-480). */
+int cbp_read_statistics(cbp_context* ctx, float* recs, size_t nmax, size_t* npass);
+
 /* Backtrack codes of the last slab's phase-1 DP, btck[r * ld + c]
  * (0 stop, 1 left, 2 up, 3 diagonal; src/libmycu/cudp/CuBatchDP_com.h:101-106). */
 int cbp_read_btck(cbp_context* ctx, uint8_t* btck, size_t ld);

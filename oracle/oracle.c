@@ -328,7 +328,8 @@ static float orc_cvs_cell(const orc_score_params* prm, long long r, long long Lq
     const float b = prm->d_cvnorm2[c] + 1.0f + lokappa0;
     const float det = fmaf(a, b, -(dot * dot));
     const float lg = logf(det);
-    const float qp = prm->q_cvprior[r], dp = prm->d_cvprior[c];
+    float qp = prm->q_cvprior[r], dp = prm->d_cvprior[c];
+    if (prm->cvs_int_priors) { qp = (float)(int)qp; dp = (float)(int)dp; }
     const float lo = fmaf(pownu0, lg, cterm) - qp - dp;
     const float v = orc_cvs_lookup(prm, lo);
     if (ambiguous) {

@@ -52,6 +52,7 @@ typedef struct orc_score_params {
     /* optional [Lq][ld] output: 1 where the map lookup of the cell would
      * change within the error bound of the reference's fast logarithm */
     uint8_t* cvs_ambiguous;
+    int cvs_int_priors;           /* MAPALN=0: log priors truncated to integers (FtorRoundMAPALN0) */
 } orc_score_params;
 
 /* constants of the context-vector score (src/libpro/srcpro/TCTXVECT.cpp:26-60) */
@@ -193,6 +194,14 @@ typedef struct orc_map_out {
 } orc_map_out;
 
 int orc_map_pair(const orc_map_in* in, orc_map_out* out);
+
+/* MAPALN=0 (FinalizeDP_ALN, src/libmycu/cudp/CuBatchDP_aln_final.cu:40-430):
+ * the alignment of the pair from its phase-1 backtrack codes btck1 ([Lq][ldb],
+ * the pair's first column first), starting at the phase-1 maximum's
+ * coordinates when that maximum is positive, else at the origin. Uses in->S,
+ * lds, the residues and SS codes; out->fb and out->btck are not touched. */
+int orc_aln_pair(const orc_map_in* in, const uint8_t* btck1, long long ldb, float maxsc,
+                 uint32_t maxcoords, orc_map_out* out);
 
 /* out4 = lambda_est, K_est, log E, log E per pair */
 void orc_significance(const orc_sig_params* sp, int Lq, int Ld, float qeno, float deno,

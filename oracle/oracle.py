@@ -103,7 +103,8 @@ class ScoreParams(ctypes.Structure):
                 ("d_cvnorm2", ctypes.c_void_p),
                 ("cvs_scores", ctypes.c_void_p), ("cvs_card", ctypes.c_int),
                 ("cvs_shift", ctypes.c_int), ("cvs_key_first", ctypes.c_float),
-                ("cvs_key_last", ctypes.c_float), ("cvs_ambiguous", ctypes.c_void_p)]
+                ("cvs_key_last", ctypes.c_float), ("cvs_ambiguous", ctypes.c_void_p),
+                ("cvs_int_priors", ctypes.c_int)]
 
 
 def load_cvs_map(path=None):
@@ -141,14 +142,16 @@ def ddms_cell(qlist: np.ndarray, dlist: np.ndarray, dstsegm: int = 6, ddmswgt: f
 
 
 def score_matrix(query, db, ss_table, ssswgt=0.12, ddmswgt=0.2, dstsegm=6, initshift=0.002,
-                 col0=0, ncols=None, nthreads=1, cvswgt=0.0, cvs_map=None, ambiguous=False):
+                 col0=0, ncols=None, nthreads=1, cvswgt=0.0, cvs_map=None, ambiguous=False,
+                 mapaln=True):
     """(scores, modscores) [Lq][ncols] for query vs db columns [col0, col0+ncols).
 
     With cvswgt > 0 the context-vector term is added (both profile sets
     must carry context vectors; the map defaults to the committed one);
     with ambiguous=True a third array [Lq][ncols] (uint8) marks the cells
     whose map lookup the reference's fast logarithm may move to a
-    neighbouring entry."""
+    neighbouring entry. mapaln=False is the MAPALN=0 configuration (the
+    caller passes initshift=0.0003; the CVS log priors are truncated)."""
     Lq = query.npositions
     N, P = db.npositions, db.nprofiles
     if ncols is None:
@@ -182,6 +185,7 @@ def score_matrix(query, db, ss_table, ssswgt=0.12, ddmswgt=0.2, dstsegm=6, inits
         prm.cvs_shift = int(m["shift"])
         prm.cvs_key_first = float(m["keys"][0])
         prm.cvs_key_last = float(m["keys"][-1])
+        prm.cvs_int_priors = 0 if mapaln else 1
         if amb is not None:
             prm.cvs_ambiguous = amb.ctypes.data
     lib().orc_score_matrix_mt(int(nthreads), Lq, q_tf.ctypes.data, q_bkg.ctypes.data,
@@ -381,6 +385,39 @@ def map_pair(query, db, p, S, M, epa, minpp=0.28, modscores=True, printsss=True)
     return {"fb": fb, "btck": bt, "aln": [b.value.decode() for b in bufs], "alnlen": mo.alnlen,
             "idts": mo.idts, "psts": mo.psts, "gaps": mo.gaps, "beg": mo.beg, "end": mo.end,
             "logz": mo.logz, "maxlogprob": mo.maxlogprob, "mapmax": mo.mapmax}
+
+
+def aln_pair(query, db, p, S, btck1, maxsc, maxr, maxc, printsss=True):
+    """MAPALN=0: the alignment of query vs profile p from the phase-1
+    backtrack codes btck1 ([Lq][Ld], the pair's columns) and the phase-1
+    maximum (raw score and its row/column). Returns the same dict fields as
+    map_pair (alignment rows, counts, coordinates)."""
+    L = lib()
+    if not getattr(L, "_aln_bound", False):
+        L.orc_aln_pair.restype = ctypes.c_int
+        L.orc_aln_pair.argtypes = [ctypes.POINTER(MapIn), ctypes.c_void_p, ctypes.c_longlong,
+                                   ctypes.c_float, ctypes.c_uint32, ctypes.POINTER(MapOut)]
+        L._aln_bound = True
+    p = int(p)
+    Lq = query.npositions
+    Ld = int(db.lens[p])
+    s0 = int(db.starts[p])
+    S = np.ascontiguousarray(S, np.float32)
+    B = np.ascontiguousarray(btck1, np.uint8)
+    qaa = np.ascontiguousarray(query.aa, np.int8)
+    daa = np.ascontiguousarray(db.aa[s0:s0 + Ld], np.int8)
+    qss = np.ascontiguousarray(query.ssstate, np.int8)
+    dss = np.ascontiguousarray(db.ssstate[s0:s0 + Ld], np.int8)
+    bufs = [ctypes.create_string_buffer(Lq + Ld + 2) for _ in range(5)]
+    mi = MapIn(Lq, Ld, S.ctypes.data, S.ctypes.data, S.shape[1], None, 0, None, 0, 0.0, 0.0, 0,
+               qaa.ctypes.data, daa.ctypes.data, qss.ctypes.data, dss.ctypes.data, int(printsss), 1, 1)
+    mo = MapOut()
+    for i in range(5):
+        mo.aln[i] = ctypes.cast(bufs[i], ctypes.c_void_p)
+    coords = ((int(maxc) & 0xffff) << 16) | (int(maxr) & 0xffff)
+    L.orc_aln_pair(ctypes.byref(mi), B.ctypes.data, B.shape[1], float(maxsc), coords, ctypes.byref(mo))
+    return {"aln": [b.value.decode() for b in bufs], "alnlen": mo.alnlen, "idts": mo.idts,
+            "psts": mo.psts, "gaps": mo.gaps, "beg": mo.beg, "end": mo.end}
 
 
 # ---------------------------------------------------------------------------

@@ -97,6 +97,9 @@ static int orc_corner_edge2(int Lq, int Ld)
     return e > 60 ? 60 : e;
 }
 
+static void orc_backtrace(const orc_map_in* in, const uint8_t* bt, long long ldb, uint32_t xx,
+                          orc_map_out* out);
+
 int orc_map_pair(const orc_map_in* in, orc_map_out* out)
 {
     const int Lq = in->Lq, Ld = in->Ld;
@@ -232,9 +235,22 @@ int orc_map_pair(const orc_map_in* in, orc_map_out* out)
     out->mapmax = best;
 
     /* ---- finalization: backtrace and alignment strings */
-    int x = 0, y = 0;
     uint32_t xx = 0;
-    if (0.0f < best) { x = bc; y = br; xx = ((uint32_t)bc << 16) | (uint32_t)br; }
+    if (0.0f < best) xx = ((uint32_t)bc << 16) | (uint32_t)br;
+    orc_backtrace(in, bt, Ld, xx, out);
+    return 0;
+}
+
+/* The finalizers' backtrace (CuBatchMAPDP_map_final.cu:150-400 and, for
+ * MAPALN=0, CuBatchDP_aln_final.cu:240-400): from the cell with
+ * coordinates xx = (x<<16)|y over the codes bt ([Lq][ldb]; 0 stop, 1 left,
+ * 2 up, 3 diagonal), the five alignment rows, identities, positives
+ * (raw score > 0), gaps and coordinates. */
+static void orc_backtrace(const orc_map_in* in, const uint8_t* bt, long long ldb, uint32_t xx,
+                          orc_map_out* out)
+{
+    const long long lds = in->lds;
+    int x = (int)(xx >> 16), y = (int)(xx & 0xffff);
     int idts = 0, psts = 0, gaps = 0, len = 0;
     char* q = out->aln[0];
     char* m = out->aln[1];
@@ -243,7 +259,7 @@ int orc_map_pair(const orc_map_in* in, orc_map_out* out)
     char* ts = out->aln[4];
     for (;;) {
         if (x < 0 || y < 0) break;
-        int b = bt[(size_t)y * Ld + x];
+        int b = bt[(size_t)y * ldb + x];
         if (b == 0) break;
         qs[len] = ' ';
         ts[len] = ' ';
@@ -284,5 +300,11 @@ int orc_map_pair(const orc_map_in* in, orc_map_out* out)
     out->gaps = gaps;
     out->beg = ((uint32_t)(x + 1) << 16) | (uint32_t)(y + 1);
     out->end = xx;
+}
+
+int orc_aln_pair(const orc_map_in* in, const uint8_t* btck1, long long ldb, float maxsc,
+                 uint32_t maxcoords, orc_map_out* out)
+{
+    orc_backtrace(in, btck1, ldb, 0.0f < maxsc ? maxcoords : 0u, out);
     return 0;
 }

@@ -13,6 +13,8 @@
 //                  block diagonals) and FinalizeDP, :330-380
 //   statistics     src/libmycu/cuss/CuBatchSS.cu:60-160 (dynamic-parallel
 //                  CalcStatisticsDynPlm, one parent thread per passed pair)
+//   MAPALN=0       FinalizeDP_ALN on the phase-1 backtrack codes
+//                  (src/libmycu/cudp/CuBatchDP.cu:427-530) instead of MAP
 //   MAP            src/libmycu/cumapdp/CuBatchMAPDP.cu:130-330 (the host
 //                  loop of its #else branch: the same kernels, in the same
 //                  order, on one stream, as its parent kernel launches them)
@@ -64,6 +66,7 @@
 #include "libmycu/cudp/CuBatchDP_com.h"
 #include "libmycu/cudp/CuBatchDP_init_btck.cuh"
 #include "libmycu/cudp/CuBatchDP_final.cuh"
+#include "libmycu/cudp/CuBatchDP_aln_final.cuh"
 #include "libmycu/cuss/CuBatchSS_com.h"
 #include "libmycu/cuss/CuBatchSS_dynplm.cuh"
 #include "libmycu/cumapdp/CuBatchMAPDP_com.h"
@@ -187,6 +190,8 @@ typedef struct refgpu_job {
     const float* cvskeys;
     const float* cvsscores;
     int cvscard;
+    // MAPALN=0: the phase-1 alignments (FinalizeDP_ALN) instead of MAP
+    int nomapaln;
 } refgpu_job;
 
 int refgpu_run(refgpu_job* J)
@@ -297,7 +302,13 @@ int refgpu_run(refgpu_job* J)
         const size_t oSS2End = oDP2FwdEnd + szss2;
         const size_t oAlnEnd = oSS2End + szaln;
         const size_t oAlnsEnd = oAlnEnd + szalns;
-        size_t oGlob = oAlnsEnd;
+        // without MAP the SS and alignment division follows the phase-1
+        // division instead of overlapping it (CuDeviceMemory.cuh:755-790)
+        const size_t oSS2Base0 = oDPBtEnd;
+        const size_t oSS2End0 = oSS2Base0 + szss2;
+        const size_t oAlnEnd0 = oSS2End0 + szaln;
+        const size_t oAlnsEnd0 = oAlnEnd0 + szalns;
+        size_t oGlob = J->nomapaln ? oAlnsEnd0 : oAlnsEnd;
         if (oGlob < oDPBtEnd)
             oGlob = oDPBtEnd;
         const size_t heapsz = oGlob + szglb + (1 << 20);
@@ -359,13 +370,21 @@ int refgpu_run(refgpu_job* J)
         dim3 sblk((unsigned)((N + 2 * sthr.x - 1) / (2 * sthr.x)),
                   (unsigned)((Lq + sthr.y - 1) / sthr.y), 1);
         CalcSM_Init_SMEMUnroll2x<<<sblk, sthr>>>(nq, n1, nC, pad, 0, 0, 0,
-                                                  CONSTINITSHIFT_MAPALN1, scores, NULL);
+                                                  J->nomapaln ? CONSTINITSHIFT_MAPALN0
+                                                              : CONSTINITSHIFT_MAPALN1,
+                                                  scores, NULL);
         ck_launch("init scores");
         FtorRoundMAPALN1 ftor_mapaln1;
+        FtorRoundMAPALN0 ftor_mapaln0;
         if (J->ssswgt > 0.0f && J->cvswgt > 0.0f) {
-            CalcSM_SSSS_CVS2S_SMEMUnroll2x<<<sblk, sthr, ssattr.szalloc_ + cvattr.szalloc_>>>(
-                d_ss, ssattr, J->ssswgt, d_cvs, cvattr, J->cvswgt, nq, n1, nC, pad, 0, 0, 0,
-                ftor_mapaln1, scores, modscores);
+            if (J->nomapaln)
+                CalcSM_SSSS_CVS2S_SMEMUnroll2x<<<sblk, sthr, ssattr.szalloc_ + cvattr.szalloc_>>>(
+                    d_ss, ssattr, J->ssswgt, d_cvs, cvattr, J->cvswgt, nq, n1, nC, pad, 0, 0, 0,
+                    ftor_mapaln0, scores, modscores);
+            else
+                CalcSM_SSSS_CVS2S_SMEMUnroll2x<<<sblk, sthr, ssattr.szalloc_ + cvattr.szalloc_>>>(
+                    d_ss, ssattr, J->ssswgt, d_cvs, cvattr, J->cvswgt, nq, n1, nC, pad, 0, 0, 0,
+                    ftor_mapaln1, scores, modscores);
             ck_launch("SS+CVS scores");
         } else if (J->ssswgt > 0.0f) {
             CalcSM_SSSS_SMEMUnroll2x<<<sblk, sthr, ssattr.szalloc_>>>(
@@ -375,8 +394,14 @@ int refgpu_run(refgpu_job* J)
             // the reference adds into modular scores it never initialised;
             // start them at zero here
             ck(cudaMemset(modscores, 0, Lq * dblen * sizeof(float)), "modscores");
-            CalcSM_CVS2S_SMEMUnroll2x<<<sblk, sthr, cvattr.szalloc_>>>(
-                d_cvs, cvattr, J->cvswgt, nq, n1, nC, pad, 0, 0, 0, ftor_mapaln1, scores, modscores);
+            if (J->nomapaln)
+                CalcSM_CVS2S_SMEMUnroll2x<<<sblk, sthr, cvattr.szalloc_>>>(
+                    d_cvs, cvattr, J->cvswgt, nq, n1, nC, pad, 0, 0, 0, ftor_mapaln0, scores,
+                    modscores);
+            else
+                CalcSM_CVS2S_SMEMUnroll2x<<<sblk, sthr, cvattr.szalloc_>>>(
+                    d_cvs, cvattr, J->cvswgt, nq, n1, nC, pad, 0, 0, 0, ftor_mapaln1, scores,
+                    modscores);
             ck_launch("CVS scores");
         }
         if (J->ddmswgt > 0.0f) {
@@ -440,8 +465,8 @@ int refgpu_run(refgpu_job* J)
             throw Fail{"more passed profiles than profiles"};
 
         // --- statistics
-        float* ss2 = (float*)(H + oDP2FwdEnd);
-        float* alndat = (float*)(H + oSS2End);
+        float* ss2 = (float*)(H + (J->nomapaln ? oSS2Base0 : oDP2FwdEnd));
+        float* alndat = (float*)(H + (J->nomapaln ? oSS2End0 : oSS2End));
         ck(cudaEventRecord(ev.e[2]), "event");
         CalcStatisticsDynPlm<<<(unsigned)npass, 1>>>(
             J->xuninf != 0, 0, 0, 0, nq, n1, nC, pad, 0, 0, 0, J->ssemodel, J->qyeno,
@@ -463,6 +488,25 @@ int refgpu_run(refgpu_job* J)
             throw Fail{"alignment buffer too small"};
         if (nposits + dbxpad2 > dp2n + 64)
             throw Fail{"phase-2 positions exceed the planned sections"};
+        if (J->nomapaln) {
+            // MAPALN=0 (CuBatchDP::FinalizeALNDynProgDevice, CuBatchDP.cu:427-530)
+            char* outalns = H + oAlnEnd0;
+            ck(cudaEventRecord(ev.e[3]), "event");
+            FinalizeDP_ALN<<<(unsigned)npass, CUDP_2DCACHE_DIM_D>>>(
+                J->ssswgt > 0.0f, J->logevthld, 0, 0, 0, 0, nq, n1, nC, pad, 0, 0, 0, dblen2,
+                (uint)dbxpad2, (uint)dbalnlen2, scores, (const float*)(H + oR),
+                (const uint*)(H + oDPBotEnd), (const char*)(H + oDPMaxEnd), alndat, outalns);
+            ck_launch("ALN finalize");
+            ck(cudaEventRecord(ev.e[4]), "event");
+            ck(cudaDeviceSynchronize(), "ALN finalize");
+            ck(cudaEventElapsedTime(&J->stage_ms[3], ev.e[3], ev.e[4]), "event time");
+            ck(cudaMemcpy(J->final_recs, alndat, npass * nTDP2OutputAlnData * sizeof(float),
+                          cudaMemcpyDeviceToHost), "final records");
+            for (int r = 0; r < nTDP2OutputAlignmentSSS; r++)
+                ck(cudaMemcpy(J->alns + (size_t)r * J->alns_cap, outalns + (size_t)r * dbalnlen2,
+                              dbalnlen2, cudaMemcpyDeviceToHost), "alignments");
+            return 0;
+        }
         {
             float* diag = (float*)(H + oR);
             float* bot = (float*)(H + oDP2DiagEnd);

@@ -54,6 +54,11 @@ CASES = {
                 xuninf=1, full=True, inputs="q64cv"),
     "cvs_only": dict(ssswgt=0.0, cvswgt=0.15, ddmswgt=0.2, dstsegm=6, minpp=0.28, ssemodel=2,
                      xuninf=1, full=True, inputs="q64cv"),
+    # MAPALN=0: the phase-1 alignments are reported (no MAP realignment)
+    "mapaln0": dict(ssswgt=0.12, ddmswgt=0.2, dstsegm=6, minpp=0.28, ssemodel=2, xuninf=1,
+                    full=True, nomapaln=1),
+    "mapaln0_cvs": dict(ssswgt=0.12, cvswgt=0.15, ddmswgt=0.2, dstsegm=6, minpp=0.28, ssemodel=2,
+                        xuninf=1, full=True, inputs="q64cv", nomapaln=1),
 }
 # every profile passes phase 1, so that each one's phase-1 record and
 # statistics are pinned; MAP realigns the pairs with log E <= LOGE_THLD
@@ -124,7 +129,7 @@ class Job(ctypes.Structure):
         ("globvars", ctypes.c_uint * 4), ("dblen", ctypes.c_int), ("dbalnlen2", ctypes.c_size_t),
         ("copy_matrices", ctypes.c_int), ("stage_ms", ctypes.c_float * 4),
         ("cvswgt", ctypes.c_float), ("cvskeys", ctypes.c_void_p), ("cvsscores", ctypes.c_void_p),
-        ("cvscard", ctypes.c_int),
+        ("cvscard", ctypes.c_int), ("nomapaln", ctypes.c_int),
     ]
 
 
@@ -159,6 +164,7 @@ def run_case(L, q, db, opts):
     cvkeys = np.ascontiguousarray(cvs["keys"], np.float32)
     cvscores = np.ascontiguousarray(cvs["scores"], np.float32)
     j.cvswgt = opts.get("cvswgt", 0.0)
+    j.nomapaln = int(opts.get("nomapaln", 0))
     j.cvskeys, j.cvsscores, j.cvscard = cvkeys.ctypes.data, cvscores.ctypes.data, len(cvkeys)
     sc = np.zeros((Lq, dblen), np.float32)
     ms = np.zeros((Lq, dblen), np.float32)

@@ -108,3 +108,32 @@ def test_map_multislab_offsets(oracle_lib, ss_table):
     assert one.alignments(q.npositions) == many.alignments(q.npositions)
     one.close()
     many.close()
+
+
+def test_mapaln0_reports_phase1_alignments(oracle_lib, ss_table):
+    """MAPALN=0: the pairs within the E-value threshold get their phase-1
+    alignment (from the phase-1 maximum over the phase-1 backtrack codes),
+    in the same rows and record fields as the MAP path."""
+    import cother_b200 as cb
+    from cother_b200 import synth
+    q, db = synth.make_workload("q200_db1k", seed=6, ndb=40, homologs=0.25)
+    bp = _search(q, db, ss_table, mapaln=0)
+    recs = cb.records_table(bp.hit_records())
+    alns = bp.alignments(q.npositions)
+    sc, _, _ = bp.read_score_matrix(q.npositions, db.npositions)
+    rec1, bt1 = oracle_lib.dp1(q, db, sc, 0, 0, db.nprofiles, -1.0e30)
+    n = 0
+    for k in range(len(recs["score"])):
+        p = int(recs["org_pro_no"][k])
+        if alns[k] is None:
+            continue
+        s0, Ld = int(db.starts[p]), int(db.lens[p])
+        o = oracle_lib.aln_pair(q, db, p, sc[:, s0:s0 + Ld], bt1[:, s0:s0 + Ld], rec1["maxsc"][p],
+                                rec1["maxr"][p], rec1["maxc"][p])
+        assert alns[k] == tuple(o["aln"]), p
+        assert (recs["identities"][k], recs["psts"][k], recs["gaps"][k]) == \
+            (o["idts"], o["psts"], o["gaps"]), p
+        assert (recs["beg_coords"][k], recs["end_coords"][k]) == (o["beg"], o["end"]), p
+        n += 1
+    assert n >= 8
+    bp.close()

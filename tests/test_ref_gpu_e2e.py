@@ -42,6 +42,7 @@ def test_search_matches_reference_kernels(case, ss_table):
     o.ssswgt, o.ddmswgt, o.dstsegm = opts["ssswgt"], opts["ddmswgt"], opts["dstsegm"]
     o.minpp, o.ssemodel, o.x_uninf = opts["minpp"], opts["ssemodel"], opts["xuninf"]
     o.cvswgt = opts.get("cvswgt", 0.0)
+    o.mapaln = 0 if opts.get("nomapaln", 0) else 1
     with cb.BatchProcessing(ss_table, o) as bp:
         if o.cvswgt > 0:
             m = np.load(os.path.join(GOLDEN, "cvs2s.npz"))

@@ -14,7 +14,8 @@ E-values), so that every comparison isolates one stage:
 * statistics: min/max exactly, lambda, K, H, E, log E and the SS18/observed
   estimates within 1e-4 relative (the reference uses __expf/__logf);
 * MAP: the set of realigned pairs, alignment rows, identity/positive/gap
-  counts, coordinates and alignment lengths exactly.
+  counts, coordinates and alignment lengths exactly; under MAPALN=0 the same
+  for the phase-1 alignments the reference reports instead.
 
 CPU only: nothing here needs a GPU.
 """
@@ -68,9 +69,11 @@ def test_score_matrix_matches_reference_kernels(case, ss_table, oracle_lib):
     neighbouring entry; all others match bit for bit too."""
     F, opts, q, db, rs, rm = _load(case)
     cvswgt = opts.get("cvswgt", 0.0)
+    mapaln = not opts.get("nomapaln", 0)
     out = oracle_lib.score_matrix(q, db, ss_table, ssswgt=opts["ssswgt"],
                                   ddmswgt=opts["ddmswgt"], dstsegm=opts["dstsegm"],
-                                  cvswgt=cvswgt, ambiguous=cvswgt > 0)
+                                  cvswgt=cvswgt, ambiguous=cvswgt > 0, mapaln=mapaln,
+                                  initshift=0.002 if mapaln else 0.0003)
     os_, om = out[0], out[1]
     amb = out[2].astype(bool) if cvswgt > 0 else np.zeros(om.shape, bool)
     assert amb.mean() < 1e-3
@@ -131,6 +134,8 @@ def test_map_alignments_match_reference_kernels(case, oracle_lib):
     thld = float(F["logevthld"])
     nrows = 5 if opts["ssswgt"] > 0 else 3
     nmap = 0
+    if opts.get("nomapaln", 0):
+        rec1, bt1 = oracle_lib.dp1(q, db, rs, 0, 0, db.nprofiles, float(F["scorethld"]))
     for k in range(len(fin)):
         p = int(_org(fin[k:k + 1])[0])
         s0, Ld = int(db.starts[p]), int(db.lens[p])
@@ -139,9 +144,16 @@ def test_map_alignments_match_reference_kernels(case, oracle_lib):
             assert alnlen == 0, p           # not realigned
             continue
         nmap += 1
-        o = oracle_lib.map_pair(q, db, p, rs[:, s0:s0 + Ld], rm[:, s0:s0 + Ld], st[k, 9],
-                                minpp=opts["minpp"], modscores=opts["ssswgt"] > 0,
-                                printsss=opts["ssswgt"] > 0)
+        if opts.get("nomapaln", 0):
+            # MAPALN=0: the phase-1 alignment from the phase-1 maximum
+            o = oracle_lib.aln_pair(q, db, p, rs[:, s0:s0 + Ld], bt1[:, s0:s0 + Ld],
+                                    rec1["maxsc"][p], rec1["maxr"][p], rec1["maxc"][p],
+                                    printsss=opts["ssswgt"] > 0)
+        else:
+            o = oracle_lib.map_pair(q, db, p, rs[:, s0:s0 + Ld], rm[:, s0:s0 + Ld], st[k, 9],
+                                    minpp=opts["minpp"],
+                                    modscores=opts["ssswgt"] > 0 or opts.get("cvswgt", 0) > 0,
+                                    printsss=opts["ssswgt"] > 0)
         assert alnlen == o["alnlen"], p
         end = int(fin[k, 2].view(np.uint32)) + k * Lq + Ld + Lq - 1
         for r in range(nrows):

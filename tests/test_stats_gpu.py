@@ -14,7 +14,6 @@ def _run(q, db, ss, thld, ssemodel=2, db_len=None, nseqs=None):
     import cother_b200 as cb
     o = cb.Options.defaults()
     o.ssemodel = ssemodel
-    o.mapaln = 0   # keep the records as the statistics stage leaves them
     bp = cb.BatchProcessing(ss, o)
     bp.set_score_threshold(thld)
     if db_len:
@@ -27,7 +26,8 @@ def _run(q, db, ss, thld, ssemodel=2, db_len=None, nseqs=None):
 
 def _check_records(bp, oracle_lib, q, db, ssemodel, expect_min=1):
     import cother_b200 as cb
-    recs = cb.records_table(bp.hit_records())
+    # the records as the statistics stage leaves them (one slab here)
+    recs = cb.records_table(bp.read_statistics())
     n = len(recs["score"])
     assert n >= expect_min
     sc, _, first = bp.read_score_matrix(q.npositions, db.npositions)
