@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
+    ap.add_argument("--qindex", type=int, default=0,
+                    help="which of the workload's query lengths (qsweep_db50k: 0, 1, 2 = 64, 256, 1024)")
     ap.add_argument("--ndb", type=int, default=None, help="override #database profiles (testing only)")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -204,7 +206,7 @@ def run_reference(args):
     from cother_b200 import synth
     ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
     ndb = args.ndb or 200
-    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=ndb,
+    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=ndb, qindex=args.qindex,
                                 context_vectors=args.cvswgt > 0)
     vals = []
     full = synth.db_lengths(args.workload, args.seed)
@@ -285,7 +287,7 @@ def main():
     from cother_b200 import synth
     ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
     # one query for all ranks; each rank holds its own database shard
-    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=args.ndb,
+    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=args.ndb, qindex=args.qindex,
                                 db_seed=args.seed + 1000 * rank, context_vectors=args.cvswgt > 0)
     Lq, Ndb = q.npositions, db.npositions
     steps_ddms = total_ddms_steps(q, db)

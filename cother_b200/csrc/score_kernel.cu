@@ -100,6 +100,16 @@ __device__ __forceinline__ float sat_mul(float a, float b)
     asm("mul.sat.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
     return r;
 }
+__device__ __forceinline__ float sat_fma(float a, float b, float c)
+{
+    float r;
+    asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// smallest positive float: the register filter's threshold while its third
+// entry is empty (every positive candidate is at least this)
+constexpr float kTiny = 0x1p-149f;
 
 // One diagonal of the DDMS segment DP. Elements e = 0,1,... pair query list
 // element oq+e with database list element od+e (upper diagonals: oq = 0,
@@ -113,15 +123,17 @@ __device__ __forceinline__ float sat_mul(float a, float b)
 // The pair scores come pre-scaled by 2^-7, so every running sum stays in
 // [0, 1) and max(sum, 0) is one saturating add; scaling by a power of two
 // commutes exactly with IEEE rounding, so the sums are the reference's
-// times 2^-7, bit for bit. The segment length is a small exact float:
+// times 2^-7, bit for bit. An odd element's mean 0.5*(a+b) is exact once a+b
+// is rounded, so adding it is one saturating fma(0.5, a+b, sum). The segment length is a small exact float:
 // len_k = len_{k-1} * [sum_{k-1} > 0] + 1, the indicator being
 // sat(sum * 2^100) (every positive sum here is far above 2^-100). A step's
 // candidate is max_k sum_k * [len_k >= DSTSEGM] and sits at the first k that
-// attains it, which is the reference's strict "<" scan.
+// attains it, which is the reference's strict "<" scan. `thr` is
+// max(third entry's score, kTiny): a candidate below it changes nothing.
 __device__ __forceinline__ void ddms_diagonal(
     const uint8_t* __restrict__ q, const uint8_t* __restrict__ d,
     const float* __restrict__ T, int lim, int oq, int od, float nsegm1,
-    float (&ms)[3], uint32_t (&mb)[3], uint32_t (&me)[3])
+    float (&ms)[3], uint32_t (&mb)[3], uint32_t (&me)[3], float& thr)
 {
     constexpr float kBig = 0x1p100f;
     float s0 = T[q[0] * kDstCard + d[0]];
@@ -131,14 +143,12 @@ __device__ __forceinline__ void ddms_diagonal(
     for (int x = 0; x < lim; x += 4) {
         const float s2 = T[q[x + 2] * kDstCard + d[x + 2]];
         const float s4 = T[q[x + 4] * kDstCard + d[x + 4]];
-        const float s1 = 0.5f * (s0 + s2);
-        const float s3 = 0.5f * (s2 + s4);
         const float l1 = __fmaf_rn(ls, sat_mul(t, kBig), 1.0f);
-        const float t1 = sat_add(t, s1);
+        const float t1 = sat_fma(0.5f, s0 + s2, t);
         const float l2 = __fmaf_rn(l1, sat_mul(t1, kBig), 1.0f);
         const float t2 = sat_add(t1, s2);
         const float l3 = __fmaf_rn(l2, sat_mul(t2, kBig), 1.0f);
-        const float t3 = sat_add(t2, s3);
+        const float t3 = sat_fma(0.5f, s2 + s4, t2);
         const float l4 = __fmaf_rn(l3, sat_mul(t3, kBig), 1.0f);
         const float t4 = sat_add(t3, s4);
         const float v1 = t1 * sat_add(l1, nsegm1);
@@ -148,12 +158,13 @@ __device__ __forceinline__ void ddms_diagonal(
         const float scom = fmaxf(fmaxf(v1, v2), fmaxf(v3, v4));
         // the register is sorted by score, so a candidate below its third
         // entry changes nothing (every branch of register_max fails)
-        if (scom != 0.0f && ms[2] <= scom) {
+        if (thr <= scom) {
             const int k = (v1 == scom) ? 1 : (v2 == scom) ? 2 : (v3 == scom) ? 3 : 4;
             const float lk = (v1 == scom) ? l1 : (v2 == scom) ? l2 : (v3 == scom) ? l3 : l4;
             const uint32_t be = (uint32_t)(x + k);
             const uint32_t bb = be + 1u - (uint32_t)lk;
             register_max(ms, mb, me, scom, cbase + bb * 0x00010001u, cbase + be * 0x00010001u);
+            thr = fmaxf(ms[2], kTiny);
         }
         s0 = s4;
         t = t4;
@@ -171,10 +182,11 @@ __device__ __forceinline__ float ddms_cell(const uint8_t* __restrict__ q, int le
     uint32_t mb[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
     uint32_t me[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
     const float nsegm1 = -(float)(dstsegm - 1);
+    float thr = kTiny;
     for (int j = len2 >> 2; 0 <= j; j -= 2)
-        ddms_diagonal(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mb, me);
+        ddms_diagonal(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mb, me, thr);
     for (int i = len1 >> 2; 0 < i; i -= 2)
-        ddms_diagonal(q + i, d, T, min(len2, len1 - i), i, 0, nsegm1, ms, mb, me);
+        ddms_diagonal(q + i, d, T, min(len2, len1 - i), i, 0, nsegm1, ms, mb, me, thr);
     float sum = 0.0f;
     sum = sum + ms[0];
     sum = sum + ms[1];
