@@ -75,6 +75,7 @@ def load_library(path: str | None = None):
         "cbp_set_logE_threshold": (i32, [vp, f32]),
         "cbp_set_cvs2s_map": (i32, [vp, vp, vp, sz]),
         "cbp_read_statistics": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
+        "cbp_get_capacities": (i32, [vp, sz, sz] + [ctypes.POINTER(sz)] * 4),
         "cbp_transfer_chunk": (i32, [vp, vp, vp, vp]),
         "cbp_process": (i32, [vp, i32, sz, vp, vp]),
         "cbp_wait_idle": (i32, [vp]),
@@ -211,6 +212,15 @@ class BatchProcessing:
 
     def set_logE_threshold(self, t: float) -> None:
         _check(load_library().cbp_set_logE_threshold(self._h, float(t)))
+
+    def capacities(self, query_len: int, expected_profile_length: int = 250) -> dict:
+        """Chunk capacities for a query length (GetCurrentMaxDbPos and the
+        like): max_db_pos, max_db_pros, max_pass2_pos, max_pass2_pros."""
+        out = [ctypes.c_size_t() for _ in range(4)]
+        _check(load_library().cbp_get_capacities(self._h, int(query_len), int(expected_profile_length),
+                                                  *[ctypes.byref(x) for x in out]))
+        return dict(zip(("max_db_pos", "max_db_pros", "max_pass2_pos", "max_pass2_pros"),
+                        (x.value for x in out)))
 
     def set_cvs2s_map(self, keys, scores) -> None:
         """The context-vector score map, needed when CVSWGT > 0: keys on the

@@ -134,6 +134,13 @@ struct ProfilesStore {
     ProfilesStore(const ProfilesStore&) = delete;
     ProfilesStore& operator=(const ProfilesStore&) = delete;
     ~ProfilesStore() { release(); }
+    size_t bytes() const {
+        size_t n = 0;
+        for (const DevBuf* b : {&tf, &ss, &dst, &dstlen, &trn, &bkg, &eno, &plen, &pstart, &pro, &aa,
+                                &sss, &cv, &cvprior, &cvnorm2})
+            n += b->bytes;
+        return n;
+    }
     void release() {
         for (DevBuf* b : {&tf, &ss, &dst, &dstlen, &trn, &bkg, &eno, &plen, &pstart, &pro, &aa, &sss,
                           &cv, &cvprior, &cvnorm2})
@@ -612,6 +619,48 @@ int cbp_share_database(cbp_context* c, cbp_context* owner)
         CBP_CUDA(cudaStreamSynchronize(owner->stream));   // its upload has completed
         c->db = owner->db;
         c->have_db = true;
+    });
+}
+
+int cbp_get_capacities(cbp_context* c, size_t query_len, size_t expected_profile_length,
+                       size_t* max_db_pos, size_t* max_db_pros, size_t* max_pass2_pos,
+                       size_t* max_pass2_pros)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!max_db_pos || !max_db_pros || !max_pass2_pos || !max_pass2_pros)
+            throw Error(CBP_ERR_ARG, "null output pointer");
+        if (query_len < 1 || query_len > (size_t)INT32_MAX || expected_profile_length < 1)
+            throw Error(CBP_ERR_ARG, "invalid query or profile length");
+        *max_db_pos = *max_db_pros = *max_pass2_pos = *max_pass2_pros = 0;
+        const int Lq = (int)query_len;
+        const size_t slab = slab_fixed_bytes(Lq) + slab_bytes_per_position(c->opt, Lq) * expected_profile_length;
+        if (slab > c->mem_budget) return;
+        // resident bytes of a chunk, as upload_profiles stores it: per
+        // position target frequencies, SS, transitions, packed distances,
+        // list length, profile index, residue, SS state (and context
+        // vectors); per profile its beginning transitions, background,
+        // ENO, length and offset
+        size_t per_pos = kNAA * 4 + kNSS * 4 + kNTrn * 4 + kDstStride + 1 + 4 + 1 + 1;
+        if (c->opt.cvswgt > 0.0f) per_pos += (kNCV + 2) * 4;
+        const size_t per_prof = kNTrn * 4 + kNAA * 4 + 4 + 4 + 8;
+        CBP_CUDA(cudaSetDevice(c->device));
+        size_t free_b = 0, total_b = 0;
+        CBP_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        size_t held_working = 0;
+        for (const DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax,
+                                &c->dpcoords, &c->dprecs, &c->passidx, &c->passdst, &c->passcnt,
+                                &c->hitrecs, &c->statrecs, &c->cs2, &c->fb2, &c->sg2, &c->bt2,
+                                &c->strip2, &c->maperr, &c->alnbuf})
+            held_working += b->bytes;
+        const size_t held_chunk = (c->db.use_count() == 1) ? c->db->bytes() : 0;
+        const size_t still = c->mem_budget > held_working ? c->mem_budget - held_working : 0;
+        const long long avail = (long long)free_b + (long long)held_chunk - (long long)still -
+                                (long long)(total_b / 100);
+        if (avail <= 0) return;
+        const size_t pros = (size_t)avail / (per_prof + expected_profile_length * per_pos);
+        *max_db_pros = *max_pass2_pros = pros;
+        *max_db_pos = *max_pass2_pos = pros * expected_profile_length;
     });
 }
 

@@ -134,6 +134,22 @@ int cbp_share_database(cbp_context* ctx, cbp_context* owner);
  * reference, whose CuDeviceMemory does the same internally). */
 int cbp_device_memory(int device, size_t* free_bytes, size_t* total_bytes);
 
+/* Chunk capacities for a query of `query_len` positions (the read-backs
+ * GetCurrentMaxDbPos, GetCurrentMaxNDbPros, GetCurrentMaxDbPosPass2 and
+ * GetCurrentMaxNDbProsPass2, src/libmycu/cupro/CuBatchProcessing.cuh:106-111,
+ * with which the reference's dispatcher sizes the chunks it reads,
+ * src/libmycu/cualn/JobDispatcher.cpp:1054-1067). A chunk fits when its
+ * resident copy fits the device memory left beside this context's working
+ * budget: with profiles of `expected_profile_length` positions on average
+ * (the reference's DEV_EXPCT_DBPROLEN), at most *max_db_pros profiles and
+ * *max_db_pos positions. The working memory is planned per slab inside the
+ * chunk with every profile allowed to pass phase 1, so the phase-2 limits
+ * equal the chunk's. All four are 0 when the budget cannot hold one slab of
+ * one such profile for this query. */
+int cbp_get_capacities(cbp_context* ctx, size_t query_len, size_t expected_profile_length,
+                       size_t* max_db_pos, size_t* max_db_pros, size_t* max_pass2_pos,
+                       size_t* max_pass2_pros);
+
 /* The context-vector score map (the reference's CVS2Scores, read from
  * src/env/cvs2s and handed to CuDeviceMemory::CacheCVS2Scores,
  * src/libmycu/cupro/CuDeviceMemory.cu:214-219, 691-740): `card` keys on the

@@ -120,3 +120,22 @@ def test_bad_inputs_fail_loudly(ss_table):
         db.dd[0, 3] = 150.0  # distance count beyond 99
         with pytest.raises(cb.CbpError):
             bp.transfer_cpm_data(db)
+
+
+def test_capacities_report_a_chunk_that_fits(ss_table):
+    """The chunk capacities (the reference's GetCurrentMaxDbPos and the like):
+    positive with a generous budget, positions = profiles x the expected
+    length, phase-2 limits equal to the chunk's, zero when the working budget
+    cannot hold one slab, and unchanged by the context's own resident chunk."""
+    import cother_b200 as cb
+    from cother_b200 import synth
+    with cb.BatchProcessing(ss_table, dev_mem_bytes=1 << 30) as bp:
+        c = bp.capacities(400, 250)
+        assert c["max_db_pros"] > 1000 and c["max_db_pos"] == 250 * c["max_db_pros"]
+        assert c["max_pass2_pos"] == c["max_db_pos"] and c["max_pass2_pros"] == c["max_db_pros"]
+        assert bp.capacities(400, 500)["max_db_pros"] < c["max_db_pros"]
+        bp.transfer_cpm_data(synth.make_profiles([300] * 20, 61, False))
+        c2 = bp.capacities(400, 250)
+        assert abs(c2["max_db_pros"] - c["max_db_pros"]) <= 0.01 * c["max_db_pros"]
+    with cb.BatchProcessing(ss_table, dev_mem_bytes=1 << 16) as bp:
+        assert bp.capacities(400, 250)["max_db_pos"] == 0
