@@ -188,7 +188,7 @@ struct cbp_context {
     int cvs_card = 0, cvs_shift = 0;
     float cvs_key_first = 0.f, cvs_key_last = 0.f;
     // working buffers
-    DevBuf scores, modscores, btck, bandbuf, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
+    DevBuf scores, modscores, btck, bandbuf, colorder, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
     DevBuf hitrecs, statrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf;
     std::vector<char> h_alns[5];
     long long base_len = 0, base_npass = 0;   // running phase-2 offsets over slabs
@@ -380,8 +380,9 @@ void check_ctx(cbp_context* c)
 }
 
 // Working bytes per slab position for a query of length Lq: score matrix,
-// modular scores and phase-1 backtrack per query row (9 Lq), the phase-1
-// band strip and per-profile records (168), and the phase-2 buffers for the
+// modular scores and phase-1 backtrack per query row (9 Lq), the score
+// kernel's column order, the phase-1 band strip and per-profile records
+// (172), and the phase-2 buffers for the
 // worst case of every profile realigned: cell scores and forward-backward
 // values per row of the padded bands (8 x 32 nb), backtrack and sign words
 // per band (12 nb), band edges (4 x 48) and alignment rows (5, plus the 5 Lq
@@ -390,7 +391,7 @@ void check_ctx(cbp_context* c)
 size_t slab_bytes_per_position(const cbp_options& o, int Lq)
 {
     const size_t nb = (size_t)map_bands(Lq);
-    size_t b = (size_t)Lq * 9 + 168 + nb * (8 * 32 + 12) + 4 * kMapMaxWarps * kMapEdgeFields + 5 +
+    size_t b = (size_t)Lq * 9 + 172 + nb * (8 * 32 + 12) + 4 * kMapMaxWarps * kMapEdgeFields + 5 +
                (size_t)Lq * 5;
     if (o.tc_form != CBP_TC_PLAIN) b += 2 * tc_operand_bytes(o.tc_form, 1);
     return b;
@@ -744,6 +745,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         c->modscores.reserve((size_t)Lq * maxcols * sizeof(float));
         c->btck.reserve((size_t)Lq * maxcols);
         c->bandbuf.reserve(5 * maxcols * sizeof(float));
+        c->colorder.reserve(maxcols * sizeof(int));
         c->dpmax.reserve(maxprof * sizeof(float));
         c->dpcoords.reserve(maxprof * sizeof(uint32_t));
         c->dprecs.reserve(maxprof * sizeof(Dp1Rec));
@@ -777,6 +779,9 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             a.dmstab = c->dmstab.as<float>();
             a.scores = c->scores.as<float>();
             a.modscores = c->modscores.as<float>();
+            a.colorder = c->colorder.as<int>();
+            CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
+            launch_column_order(c->db->view.dstlen, s.col0, s.ncols, a.ld, c->colorder.as<int>(), c->stream);
             if (c->opt.tc_form != CBP_TC_PLAIN) {
                 if (!c->cublas) {
                     if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS)
@@ -797,6 +802,8 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 tc_profile_sums(t, f, c->cublas, c->tcq_hi.p, c->tcq_lo.p, c->tcd_hi.p, c->tcd_lo.p,
                                 a.scores, c->stream);
                 a.dots_in_scores = true;
+                c->launches += 2;   // the two operand-split kernels (the GEMMs are cuBLAS's)
+                c->stage_launches[0] += 2;
             }
 
             Dp1Args d;
@@ -814,7 +821,6 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             d.maxcoords = c->dpcoords.as<uint32_t>();
             d.recs = c->dprecs.as<Dp1Rec>();
 
-            CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
             launch_score_matrix(a, c->stream);
             CBP_CUDA(cudaEventRecord(c->ev[1], c->stream));
             launch_dp1(d, c->stream);
@@ -823,8 +829,8 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             launch_pass_compact(d, c->passidx.as<int>(), c->passdst.as<long long>(), c->passcnt.as<int>(),
                                 reinterpret_cast<long long*>(c->passcnt.as<char>() + 8), c->stream);
             CBP_CUDA(cudaEventRecord(c->ev[3], c->stream));
-            c->launches += 4;
-            c->stage_launches[0] += 1;
+            c->launches += 5;
+            c->stage_launches[0] += 2;
             c->stage_launches[1] += 1;
             c->stage_launches[2] += 2;
             int npass = 0;

@@ -59,12 +59,13 @@ __device__ __forceinline__ bool seg_intersect(uint32_t b1, uint32_t e1, uint32_t
     const uint32_t mx = vmax_u16x2(b1, b2), mn = vmin_u16x2(e1, e2);
     return ((mn + 0x01000100u - mx) & 0xff00ff00u) != 0u;
 }
+// The update proper, for a candidate s >= ms[2] whose intersection with the
+// top entry (x0) is known and that changes the register: s >= ms[0] or not
+// x0. Every case of the reference's register tests the candidate against
+// the entries at ranks 0 and 1 (an empty entry's test never matters).
 __device__ __forceinline__ void register_max(float (&ms)[3], uint32_t (&mb)[3], uint32_t (&me)[3],
-                                             float s, uint32_t cb, uint32_t ce)
+                                             float s, uint32_t cb, uint32_t ce, bool x0)
 {
-    // every case of the reference's register tests the candidate against
-    // the entries at ranks 0 and 1 (an empty entry's test never matters)
-    const bool x0 = seg_intersect(cb, ce, mb[0], me[0]);
     const bool x1 = seg_intersect(cb, ce, mb[1], me[1]);
     if (ms[0] <= s) {
         const float a1 = x0 ? 0.0f : ms[0];
@@ -76,13 +77,11 @@ __device__ __forceinline__ void register_max(float (&ms)[3], uint32_t (&mb)[3], 
         mb[2] = mb[1]; me[2] = me[1];
         mb[1] = b1; me[1] = e1;
         ms[0] = s; mb[0] = cb; me[0] = ce;
-    } else if (ms[1] <= s) {
-        if (!x0) {
-            ms[2] = x1 ? 0.0f : ms[1]; mb[2] = mb[1]; me[2] = me[1];
-            ms[1] = s; mb[1] = cb; me[1] = ce;
-        }
-    } else if (ms[2] <= s) {
-        if (!x0 && !x1) { ms[2] = s; mb[2] = cb; me[2] = ce; }
+    } else if (ms[1] <= s) {          // not x0 here
+        ms[2] = x1 ? 0.0f : ms[1]; mb[2] = mb[1]; me[2] = me[1];
+        ms[1] = s; mb[1] = cb; me[1] = ce;
+    } else if (!x1) {                 // ms[2] <= s, not x0
+        ms[2] = s; mb[2] = cb; me[2] = ce;
     }
 }
 
@@ -160,11 +159,26 @@ __device__ __forceinline__ void ddms_diagonal(
         // entry changes nothing (every branch of register_max fails)
         if (thr <= scom) {
             const int k = (v1 == scom) ? 1 : (v2 == scom) ? 2 : (v3 == scom) ? 3 : 4;
-            const float lk = (v1 == scom) ? l1 : (v2 == scom) ? l2 : (v3 == scom) ? l3 : l4;
             const uint32_t be = (uint32_t)(x + k);
-            const uint32_t bb = be + 1u - (uint32_t)lk;
-            register_max(ms, mb, me, scom, cbase + bb * 0x00010001u, cbase + be * 0x00010001u);
-            thr = fmaxf(ms[2], kTiny);
+            uint32_t bb;
+            if (nsegm1 <= -4.0f) {
+                // DSTSEGM >= 5: the candidate, at least 5 long and ending at
+                // x+k <= x+4, contains element x, so it is the segment running
+                // at x, which began at x + 1 - ls
+                bb = (uint32_t)(x + 1) - (uint32_t)ls;
+            } else {
+                const float lk = (v1 == scom) ? l1 : (v2 == scom) ? l2 : (v3 == scom) ? l3 : l4;
+                bb = be + 1u - (uint32_t)lk;
+            }
+            const uint32_t cb = cbase + bb * 0x00010001u, ce = cbase + be * 0x00010001u;
+            // below the top entry and intersecting it, a candidate changes
+            // nothing (the reference's second and third cases both require
+            // no intersection with the top); most candidates end here
+            const bool x0 = seg_intersect(cb, ce, mb[0], me[0]);
+            if (ms[0] <= scom || !x0) {
+                register_max(ms, mb, me, scom, cb, ce, x0);
+                thr = fmaxf(ms[2], kTiny);
+            }
         }
         s0 = s4;
         t = t4;
@@ -243,6 +257,7 @@ score_matrix_kernel(const ScoreArgs a)
     __shared__ float s_dcvpn[2][kCols];       // their log priors and squared norms
     __shared__ float s_qcv[kRows][kNCV + 1];
     __shared__ float s_qcvpn[2][kRows];
+    __shared__ int s_col[kCols];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -251,12 +266,17 @@ score_matrix_kernel(const ScoreArgs a)
     const int rowb = blockIdx.y * kRows;
     const long long N = a.db.N;
 
+    if (tid < kCols) {
+        const int slot = colb + tid;
+        s_col[tid] = slot < a.ncols ? (a.colorder ? a.colorder[slot] : slot) : -1;
+    }
     for (int i = tid; i < kDstCard * kDstCard; i += kThreads) s_dms[i] = a.dmstab[i] * 0x1p-7f;
     for (int i = tid; i < kSSCard * kSSCard; i += kThreads) s_sst[i] = a.sstab[i];
+    __syncthreads();
 
-    // database columns of this block
-    const int col = colb + lane;
-    const bool cvalid = col < a.ncols;
+    // database columns of this block: lane l takes slab column s_col[l]
+    const int col = s_col[lane];
+    const bool cvalid = col >= 0;
     const long long gpos = a.col0 + col;
     if (cvalid) {
         const int p = a.db.pro[gpos];
@@ -272,9 +292,10 @@ score_matrix_kernel(const ScoreArgs a)
     // distance lists: 32 columns x 104 bytes, in 16-byte pieces
     for (int idx = tid; idx < kCols * 7; idx += kThreads) {
         const int c = idx / 7, piece = idx - c * 7;
+        const int cc = s_col[c];
         uint4 v;
-        if (colb + c < a.ncols) {
-            v = *reinterpret_cast<const uint4*>(a.db.dst + (a.col0 + colb + c) * kDstStride + piece * 16);
+        if (cc >= 0) {
+            v = *reinterpret_cast<const uint4*>(a.db.dst + (a.col0 + cc) * kDstStride + piece * 16);
         } else {
             const uint32_t f = 0x15151515u;  // kDstNoData in every byte
             v = make_uint4(f, f, f, f);
@@ -414,6 +435,49 @@ score_matrix_kernel(const ScoreArgs a)
 }
 
 }  // namespace
+
+// One block per window: a counting sort of the window's columns by
+// descending list length (0..kMaxDst). The order within one length is
+// arbitrary: it decides only which lane computes a cell, never its value.
+__global__ void __launch_bounds__(256)
+column_order_kernel(const uint8_t* __restrict__ dstlen, long long col0, int ncols, long long ld,
+                    int* __restrict__ order)
+{
+    __shared__ int s_cnt[kMaxDst + 1];
+    const int w0 = blockIdx.x * kOrderWindow;
+    const int n = min(kOrderWindow, ncols - w0);
+    for (int i = threadIdx.x; i <= kMaxDst; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        atomicAdd(&s_cnt[kMaxDst - min((int)dstlen[col0 + w0 + i], kMaxDst)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int b = 0; b <= kMaxDst; b++) {
+            const int c = s_cnt[b];
+            s_cnt[b] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int b = kMaxDst - min((int)dstlen[col0 + w0 + i], kMaxDst);
+        order[w0 + atomicAdd(&s_cnt[b], 1)] = w0 + i;
+    }
+    // slots past the last column (the final window only)
+    for (long long i = (long long)w0 + n + threadIdx.x; i < min(ld, (long long)w0 + kOrderWindow);
+         i += blockDim.x)
+        order[i] = -1;
+}
+
+void launch_column_order(const uint8_t* dstlen, long long col0, int ncols, long long ld, int* order,
+                         cudaStream_t stream)
+{
+    if (ncols <= 0) return;
+    column_order_kernel<<<(unsigned)ceil_div(ncols, kOrderWindow), 256, 0, stream>>>(dstlen, col0, ncols, ld,
+                                                                                     order);
+    CBP_CHECK_LAUNCH();
+}
 
 void launch_score_matrix(const ScoreArgs& a, cudaStream_t stream)
 {
