@@ -52,8 +52,15 @@ constexpr int kChunk = 32;              // columns per staged chunk
 constexpr int kScoreRing = 3;           // score tiles in flight per warp
 constexpr int kBtckRing = 2;            // backtrack tiles per warp
 
+// per chunk of 32 columns: the score tile, the profile transitions of the
+// chunk's columns (MI and II from the next column's entry, as the DP reads
+// them) and, for bands below the first, the previous band's bottom row from
+// the strip; all fetched with cp.async one chunk ahead, so that no step
+// waits on a global load
 struct DpStage {
     float sc[kScoreRing][32][kChunk];
+    float tr[kScoreRing][kNTrn][kChunk];
+    float sp[kScoreRing][5][kChunk];
     uint8_t bt[kBtckRing][32][kChunk];
 };
 
@@ -66,18 +73,33 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool val
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// issue the loads of score chunk k of rows r0..r0+31 (zero outside the matrix)
+// issue the loads of chunk k for the band of rows r0..r0+31: its score
+// tile (zero outside the matrix), the transitions of its columns and, below
+// the first band, the strip (the previous band's bottom row)
 __device__ __forceinline__ void fetch_chunk(DpStage& st, const float* __restrict__ S, long long ld,
-                                            int r0, int Lq, int Ld, int k, int lane)
+                                            int r0, int Lq, int Ld, int k, int lane,
+                                            const float* __restrict__ trn, long long NT, long long tb,
+                                            const float* __restrict__ strip)
 {
     const int c = k * kChunk + lane;
     const bool cv = c < Ld;
-    float (*tile)[kChunk] = st.sc[k % kScoreRing];
+    const int slot = k % kScoreRing;
+    float (*tile)[kChunk] = st.sc[slot];
 #pragma unroll 4
     for (int i = 0; i < 32; i++) {
         const bool v = cv && (r0 + i < Lq);
         const float* src = v ? S + (long long)(r0 + i) * ld + c : S;
         cp_async4(&tile[i][lane], src, v);
+    }
+    const long long e = tb + c;
+#pragma unroll
+    for (int f = 0; f < kNTrn; f++) {
+        const long long ef = (f == trMI || f == trII) ? e + 1 : e;
+        cp_async4(&st.tr[slot][f][lane], cv ? trn + f * NT + ef : trn, cv);
+    }
+    if (r0 > 0) {
+#pragma unroll
+        for (int f = 0; f < 5; f++) cp_async4(&st.sp[slot][f][lane], cv ? strip + f * ld + c : strip, cv);
     }
 }
 
@@ -150,12 +172,13 @@ dp1_kernel(const Dp1Args a)
         const bool top = (r0 == 0);
         const int nsteps = Ld + 31;
         __syncwarp();   // the previous band's tiles are no longer read
-        fetch_chunk(st, S, ld, r0, Lq, Ld, 0, lane);
+        fetch_chunk(st, S, ld, r0, Lq, Ld, 0, lane, a.db.trn, NT, tb, strip);
         cp_async_commit();
         for (int s = 0; s < nsteps; s++) {
             if ((s & 31) == 0) {
                 // chunk s/32 must be resident; fetch the next one
-                if ((s >> 5) + 1 < nchunks) fetch_chunk(st, S, ld, r0, Lq, Ld, (s >> 5) + 1, lane);
+                if ((s >> 5) + 1 < nchunks)
+                    fetch_chunk(st, S, ld, r0, Lq, Ld, (s >> 5) + 1, lane, a.db.trn, NT, tb, strip);
                 cp_async_commit();
                 cp_async_wait1();
                 __syncwarp();
@@ -174,8 +197,9 @@ dp1_kernel(const Dp1Args a)
             float uND = __shfl_up_sync(kFull, lND, 1);
             if (lane == 0) {
                 if (!top && c < Ld) {
-                    uMM = strip[0 * ld + c]; uMI = strip[1 * ld + c]; uIM = strip[2 * ld + c];
-                    uDN = strip[3 * ld + c]; uND = strip[4 * ld + c];
+                    const float (*sp)[kChunk] = st.sp[(c >> 5) % kScoreRing];
+                    uMM = sp[0][c & 31]; uMI = sp[1][c & 31]; uIM = sp[2][c & 31];
+                    uDN = sp[3][c & 31]; uND = sp[4][c & 31];
                 } else {
                     uMM = uMI = uIM = uDN = uND = 0.f;
                 }
@@ -185,11 +209,12 @@ dp1_kernel(const Dp1Args a)
                 dMM = dMI = dIM = dDN = dND = 0.f;
             }
             if (rv && c >= 0 && c < Ld) {
-                const long long e = tb + c;
-                const float dMMp = a.db.trn[trMM * NT + e], dIMp = a.db.trn[trIM * NT + e];
-                const float dDMp = a.db.trn[trDM * NT + e], dMDp = a.db.trn[trMD * NT + e];
-                const float dDDp = a.db.trn[trDD * NT + e];
-                const float dMIc = a.db.trn[trMI * NT + e + 1], dIIc = a.db.trn[trII * NT + e + 1];
+                const float (*tr)[kChunk] = st.tr[(c >> 5) % kScoreRing];
+                const int cc = c & 31;
+                const float dMMp = tr[trMM][cc], dIMp = tr[trIM][cc];
+                const float dDMp = tr[trDM][cc], dMDp = tr[trMD][cc];
+                const float dDDp = tr[trDD][cc];
+                const float dMIc = tr[trMI][cc], dIIc = tr[trII][cc];
                 const float sc = in_corner(Lq, Ld, edge, r, c) ? -9.0f
                                  : st.sc[(c >> 5) % kScoreRing][lane][c & 31];
                 float v1, v2, mx;

@@ -238,7 +238,7 @@ __device__ __forceinline__ float cvs_cell(const ScoreArgs& a, const float* __res
     return __ldg(a.cvs_scores + a.cvs_shift + (int)rintf(lo + lo));
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 10)
 score_matrix_kernel(const ScoreArgs a)
 {
     __shared__ float s_dms[kDstCard * kDstCard];
@@ -253,10 +253,14 @@ score_matrix_kernel(const ScoreArgs a)
     __shared__ float s_qbg[kNAA];
     __shared__ int s_dlen[kCols];
     __shared__ int s_qlen[kRows];
-    __shared__ float s_dcv[kNCV][kCols];      // context vectors (CVSWGT > 0)
-    __shared__ float s_dcvpn[2][kCols];       // their log priors and squared norms
-    __shared__ float s_qcv[kRows][kNCV + 1];
-    __shared__ float s_qcvpn[2][kRows];
+    // context vectors and their log priors and squared norms (CVSWGT > 0):
+    // dynamic shared memory, absent otherwise, so that ten blocks fit an SM
+    extern __shared__ float s_cvsdyn[];
+    float (*s_dcv)[kCols] = reinterpret_cast<float (*)[kCols]>(s_cvsdyn);
+    float (*s_dcvpn)[kCols] = reinterpret_cast<float (*)[kCols]>(s_cvsdyn + kNCV * kCols);
+    float (*s_qcv)[kNCV + 1] = reinterpret_cast<float (*)[kNCV + 1]>(s_cvsdyn + (kNCV + 2) * kCols);
+    float (*s_qcvpn)[kRows] =
+        reinterpret_cast<float (*)[kRows]>(s_cvsdyn + (kNCV + 2) * kCols + kRows * (kNCV + 1));
     __shared__ int s_col[kCols];
 
     const int tid = threadIdx.x;
@@ -483,7 +487,9 @@ void launch_score_matrix(const ScoreArgs& a, cudaStream_t stream)
 {
     if (a.ncols <= 0 || a.Lq <= 0) return;
     dim3 grid((unsigned)ceil_div(a.ncols, kCols), (unsigned)ceil_div(a.Lq, kRows));
-    score_matrix_kernel<<<grid, kThreads, 0, stream>>>(a);
+    const size_t cvs_smem =
+        a.cvswgt > 0.0f ? sizeof(float) * ((kNCV + 2) * kCols + kRows * (kNCV + 1) + 2 * kRows) : 0;
+    score_matrix_kernel<<<grid, kThreads, cvs_smem, stream>>>(a);
     CBP_CHECK_LAUNCH();
 }
 
