@@ -99,6 +99,11 @@ def load_library(path: str | None = None):
         "cbp_stage_times": (i32, [vp, vp, i32]),
         "cbp_launch_count": (i32, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "cbp_stage_launches": (i32, [vp, vp, i32]),
+        "cbp_default_format_options": (None, [vp]),
+        "cbp_format_hits": (i32, [vp, vp, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
+        "cbp_format_hits_host": (i32, [vp, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
+        "cbp_merge_hit_lists": (i32, [sz, vp, vp, vp, vp]),
+        "cbp_write_report": (i32, [vp, vp, vp, vp, sz, vp, sz, ctypes.POINTER(sz)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -363,6 +368,12 @@ class BatchProcessing:
         b = np.zeros((nrows, max_cols), np.uint8)
         _check(load_library().cbp_read_btck(self._h, b.ctypes.data, max_cols))
         return b
+
+    def format_hits(self, descs=None, options=None):
+        """Per-hit text of the last search in the finalizer's order: a list
+        of (annotation, hit record) strings (cbp_format_hits)."""
+        from . import report
+        return report.format_hits_ctx(self._h, descs, options)
 
     def stage_times(self) -> list:
         buf = (ctypes.c_float * 6)()

@@ -34,6 +34,7 @@ CUDA_SOURCES = [
     "map_kernel.cu",
     "dp1_noalloc.cu",
     "tc_kernel.cu",
+    "format.cpp",
 ]
 CUDA_HEADERS = [
     "map_kernel.cuh",

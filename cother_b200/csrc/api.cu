@@ -24,10 +24,17 @@
 
 namespace cbp {
 
+// format.cpp: the finalizer's per-hit text from host records and rows
+int format_hits_from(const float* recs, size_t nrecs, const char* rows, size_t row_stride, size_t row_length,
+                     const int* prof_len, const float* prof_eno, const uint8_t* prof_ss, size_t nprof,
+                     const char* const* descs, int query_len, float query_eno, int query_ss, float ssswgt,
+                     float logevthld, float sspace, const cbp_format_options* fo, char* buf, size_t cap,
+                     size_t* used, size_t* nhits);
+
 // field indices (src/libmycu/cupro/PM2DVectorFields.h:51-87)
 enum {
     fBkg = 0, fENO = 20, fLen = 21, fDist = 22, fTrn = 23, fTF = 30, fCV = 50,
-    fDD = 71, fSS = 171, fAddrPro = 176, fAA = 179, fSSstate = 180, fTot = 181
+    fDD = 71, fSS = 171, fAddrPro = 176, fAddrSS = 178, fAA = 179, fSSstate = 180, fTot = 181
 };
 
 static thread_local std::string g_last_error;
@@ -130,6 +137,11 @@ struct ProfilesStore {
     ProfilesDev view;
     std::vector<int> h_plen;
     std::vector<long long> h_pstart;
+    // for the text output: ENO per profile and whether the profile carries
+    // SS data (pmv2DAddrSS of its first position is not -1; empty when the
+    // field was not given)
+    std::vector<float> h_eno;
+    std::vector<uint8_t> h_ss;
     ProfilesStore() = default;
     ProfilesStore(const ProfilesStore&) = delete;
     ProfilesStore& operator=(const ProfilesStore&) = delete;
@@ -148,6 +160,8 @@ struct ProfilesStore {
         view = ProfilesDev();
         h_plen.clear();
         h_pstart.clear();
+        h_eno.clear();
+        h_ss.clear();
     }
 };
 
@@ -293,6 +307,17 @@ void upload_profiles(ProfilesStore& st, char* const* beg, char* const* end, cuda
         acc += lens[p];
     }
     if ((size_t)acc != N) throw Error(CBP_ERR_ARG, "sum of profile lengths differs from #positions");
+    {
+        const float* eno = reinterpret_cast<const float*>(beg[fENO]);
+        if (field_bytes(beg, end, fENO) != P * sizeof(float)) throw Error(CBP_ERR_ARG, "ENO field of wrong size");
+        st.h_eno.assign(eno, eno + P);
+        st.h_ss.clear();
+        if (beg[fAddrSS] && end[fAddrSS] && (size_t)(end[fAddrSS] - beg[fAddrSS]) == N * sizeof(int)) {
+            const int* addr = reinterpret_cast<const int*>(beg[fAddrSS]);
+            st.h_ss.resize(P);
+            for (size_t p = 0; p < P; p++) st.h_ss[p] = addr[st.h_pstart[p]] != -1 ? 1 : 0;
+        }
+    }
 
     // packed distance lists
     std::vector<uint8_t> dst((size_t)N * kDstStride);
@@ -1113,6 +1138,27 @@ int cbp_get_alignments(cbp_context* c, char* rows, size_t row_stride, size_t* le
             for (int r = 0; r < 5; r++) std::memcpy(rows + (size_t)r * row_stride, c->h_alns[r].data(), n);
         }
     });
+}
+
+int cbp_format_hits(cbp_context* c, const cbp_format_options* fo, const char* const* descs, char* buf,
+                    size_t cap, size_t* used, size_t* nhits)
+{
+    int rc = CBP_OK;
+    const int grc = guarded([&] {
+        check_ctx(c);
+        if (!c->have_db) throw Error(CBP_ERR_STATE, "no database chunk transferred");
+        const ProfilesStore& db = *c->db;
+        const size_t n = c->h_alns[0].size();
+        std::vector<char> rows(5 * n);
+        for (int r = 0; r < 5; r++)
+            if (n) std::memcpy(rows.data() + (size_t)r * n, c->h_alns[r].data(), n);
+        const int qss = c->query.h_ss.empty() ? 1 : c->query.h_ss[0];
+        rc = format_hits_from(c->h_recs.data(), c->h_recs.size() / kRecFloats, rows.data(), n, n,
+                              db.h_plen.data(), db.h_eno.data(), db.h_ss.empty() ? nullptr : db.h_ss.data(),
+                              db.h_plen.size(), descs, c->last_Lq, c->query_eno, qss, c->opt.ssswgt,
+                              c->logE_thld, (float)c->searchspace, fo, buf, cap, used, nhits);
+    });
+    return grc != CBP_OK ? grc : rc;
 }
 
 int cbp_get_search_space(cbp_context* c, uint64_t* search_space, size_t* delta_length)

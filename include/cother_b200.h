@@ -266,6 +266,94 @@ int cbp_get_hit_list(cbp_context* ctx, int32_t* order, size_t max_hits, size_t* 
  * src/libpro/srcsco/AbstractScoreMatrix.cpp:247-393). */
 int cbp_get_search_space(cbp_context* ctx, uint64_t* search_space, size_t* delta_length);
 
+/* ------------------------------------------------------------------------
+ * Text output of the results: the finalizer's per-hit text and the writer's
+ * per-query report, plain (.out) or JSON (.json), in the reference's layout
+ * (CuBatchProcessingFinalizer::CompressResultsPlain/JSON,
+ * src/libmycu/cupro/CuBatchProcessingFinalizerPlain.cpp:35-385 and
+ * CuBatchProcessingFinalizerJSON.cpp:35-380; AlnWriter::WriteResultsPlain/
+ * JSON, src/libmycu/cualn/AlnWriterPlain.cpp:19-398 and AlnWriterJSON.cpp:
+ * 19-429; AlnWriter::MergeResults, src/libmycu/cualn/AlnWriter.cpp:216-256). */
+#define CBP_FORMAT_PLAIN 0
+#define CBP_FORMAT_JSON  1
+
+typedef struct cbp_format_options {
+    int format;     /* CBP_FORMAT_PLAIN or CBP_FORMAT_JSON (the reference's -f) */
+    int dsclen;     /* DSCLEN: maximum length of a description (1024) */
+    int dscwidth;   /* DSCWIDTH: width at which descriptions wrap (80) */
+    int alnwidth;   /* ALNWIDTH: alignment characters per line (60) */
+    int show;       /* SHOW: statistics footer of each plain hit record (1) */
+} cbp_format_options;
+
+/* The reference's defaults (src/env/options.txt). */
+void cbp_default_format_options(cbp_format_options* fo);
+
+/* Per-hit text of the last cbp_process() call, for the hits that
+ * cbp_get_hit_list reports and in its order: for each, the annotation line
+ * of the summary list, a NUL, the hit record (description, scores,
+ * alignment, statistics), a NUL. descs[p] is the description of chunk
+ * profile p (NULL: none). With buf == NULL only *used (bytes) and *nhits are
+ * set; a buffer smaller than *used gives CBP_ERR_LIMIT. */
+int cbp_format_hits(cbp_context* ctx, const cbp_format_options* fo, const char* const* descs,
+                    char* buf, size_t cap, size_t* used, size_t* nhits);
+
+/* The same from host data, without a context (the finalizer's inputs). */
+typedef struct cbp_hits_input {
+    const float* recs;        /* hit records, CBP_REC_FLOATS each (cbp_get_hit_records) */
+    size_t nrecs;
+    const char* rows;         /* the 5 alignment rows (cbp_get_alignments) */
+    size_t row_stride;        /* bytes from one row to the next */
+    size_t row_length;        /* bytes of each row */
+    const int* prof_len;      /* per chunk profile: length */
+    const float* prof_eno;    /* per chunk profile: effective number of observations */
+    const uint8_t* prof_ss;   /* per chunk profile: carries SS data (NULL: all do) */
+    size_t nprof;
+    const char* const* descs; /* per chunk profile: description (NULL: none) */
+    int query_len;
+    float query_eno;
+    int query_ss;             /* the query carries SS data */
+    float ssswgt;             /* SSSWGT > 0 shows the SS rows of plain records */
+    float log_evalue_threshold;
+    float search_space;       /* effective search space (bit scores) */
+} cbp_hits_input;
+int cbp_format_hits_host(const cbp_hits_input* in, const cbp_format_options* fo, char* buf,
+                         size_t cap, size_t* used, size_t* nhits);
+
+/* Merge the sorted hit lists of a query's database chunks (parts) by log
+ * E-value, stably (equal values keep part order, then list order), as the
+ * reference's writer joins them. log_evalues[p][i] is the log E-value of
+ * hit i of part p. Writes part[] and index[] (sum of counts entries each;
+ * either may be NULL). */
+int cbp_merge_hit_lists(size_t nparts, const float* const* log_evalues, const size_t* counts,
+                        int32_t* part, int32_t* index);
+
+/* What the report says besides the hits. */
+typedef struct cbp_report_info {
+    const char* program;              /* program name (NULL: none) */
+    const char* version;              /* version (NULL: none) */
+    const char* const* references;    /* NULL-terminated list of citation lines, or NULL */
+    int query_len;
+    const char* query_desc;           /* query description (NULL: none) */
+    const char* const* db_names;      /* database names */
+    size_t n_db_names;
+    uint64_t db_size;                 /* total database positions */
+    uint64_t db_entries;              /* database profiles */
+    float log_evalue_threshold;
+    float search_space;               /* effective search space */
+    int delta_length;                 /* length adjustment */
+    float ref_lambda, ref_k;          /* ungapped reference values */
+    float gapped_lambda, gapped_k;    /* gapped values */
+    int nohits;                       /* NOHITS: annotations listed */
+    int noalns;                       /* NOALNS: hit records listed */
+} cbp_report_info;
+
+/* The per-query report text from the merged hits (annotations[i],
+ * hit_records[i] in final order, as cbp_format_hits gives them). With buf ==
+ * NULL only *used is set; a smaller buffer gives CBP_ERR_LIMIT. */
+int cbp_write_report(const cbp_report_info* info, const cbp_format_options* fo,
+                     const char* const* annotations, const char* const* hit_records, size_t nhits,
+                     char* buf, size_t cap, size_t* used);
+
 /* Karlin-Altschul parameters of the statistical configuration (cother.par:
  * [UNGAPPED] lambda, K; [GAPPED_A_1] lambda, K, alpha, beta). Defaults are
  * the reference's shipped values. */
