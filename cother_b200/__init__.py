@@ -104,6 +104,12 @@ def load_library(path: str | None = None):
         "cbp_format_hits_host": (i32, [vp, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
         "cbp_merge_hit_lists": (i32, [sz, vp, vp, vp, vp]),
         "cbp_write_report": (i32, [vp, vp, vp, vp, sz, vp, sz, ctypes.POINTER(sz)]),
+        "cbp_db_open": (i32, [ctypes.c_char_p, ctypes.POINTER(vp)]),
+        "cbp_db_close": (i32, [vp]),
+        "cbp_db_info": (i32, [vp] + [ctypes.POINTER(ctypes.c_uint64)] * 3),
+        "cbp_db_profile_lengths": (i32, [vp, vp]),
+        "cbp_db_chunk": (i32, [vp, ctypes.c_uint64, ctypes.c_uint64, vp, vp, vp]),
+        "cbp_db_write": (i32, [ctypes.c_char_p, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -246,6 +252,13 @@ class BatchProcessing:
         beg, end = db.field_tables()
         _check(load_library().cbp_transfer_chunk(self._h, beg, end, None))
         self._db = db
+
+    def transfer_db_chunk(self, database, first: int, count: int):
+        """Transfer profiles first .. first+count-1 of an opened database
+        file (cother_b200.database.Database); returns their descriptions."""
+        beg, end, descs = database.chunk(first, count)
+        _check(load_library().cbp_transfer_chunk(self._h, beg, end, None))
+        return descs
 
     def share_database(self, owner: "BatchProcessing") -> None:
         """Search `owner`'s resident database (same device) without a copy."""

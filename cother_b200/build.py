@@ -35,6 +35,7 @@ CUDA_SOURCES = [
     "dp1_noalloc.cu",
     "tc_kernel.cu",
     "format.cpp",
+    "dbfile.cpp",
 ]
 CUDA_HEADERS = [
     "map_kernel.cuh",

@@ -120,6 +120,35 @@ int cbp_set_logE_threshold(cbp_context* ctx, float log_threshold);
 int cbp_transfer_chunk(cbp_context* ctx, char* const* pmbeg, char* const* pmend,
                        const size_t* szfields);
 
+/* ------------------------------------------------------------------------
+ * Binary profile database files in the reference's format v2.2 (what its
+ * db2bin writes: "COTHER profile bin database v2.5"; Db::MakeBin_v2_2,
+ * src/libpro/srcpro/Db.cpp:340-385, and BinaryWriteProfile_v2_2,
+ * src/libpro/srcpro/PMProfileModel.cpp:1250-1810), replacing the chunk
+ * reading of TdDataReader/CuDbReader (src/libmycu/cupro/TdDataReader.cpp:
+ * 387-984, CuDbReader.cpp:457-519). The file is mapped, not copied. */
+typedef struct cbp_db cbp_db;
+
+/* Open and validate a database file (signature, version, address table,
+ * section extents, profile lengths, descriptions). */
+int cbp_db_open(const char* path, cbp_db** db);
+int cbp_db_close(cbp_db* db);
+/* Number of profiles, positions and distance values (the file's header). */
+int cbp_db_info(cbp_db* db, uint64_t* nprofiles, uint64_t* npositions, uint64_t* ndistances);
+/* The lengths of all profiles (nprofiles ints), for planning chunks. */
+int cbp_db_profile_lengths(cbp_db* db, int32_t* lens);
+/* Profiles first .. first+count-1 as the 181 begin/end field pointers that
+ * cbp_transfer_chunk takes, and their descriptions (descs may be NULL; else
+ * count entries). The stored fields point into the mapped file; the derived
+ * ones (pps2DDist, pmv2DAddrPro, pmv2DAddrCV, pmv2DAddrSS) into buffers of
+ * the handle. Valid until the next cbp_db_chunk call or cbp_db_close. */
+int cbp_db_chunk(cbp_db* db, uint64_t first, uint64_t count, char** beg, char** end,
+                 const char** descs);
+/* Write profiles given as a 181-field table (one chunk: all fields of the
+ * sizes cbp_transfer_chunk expects) with their descriptions (NULL: empty)
+ * to a database file of this format. */
+int cbp_db_write(const char* path, char* const* beg, char* const* end, const char* const* descs);
+
 /* Use `owner`'s resident database chunk instead of a copy of one's own (no
  * counterpart in the reference, where each worker transfers its chunk).
  * Several contexts on one device can then search the same resident database
