@@ -45,6 +45,7 @@ class Options(ctypes.Structure):
         ("dstsegm", ctypes.c_int), ("mapaln", ctypes.c_int), ("minpp", ctypes.c_float),
         ("ssemodel", ctypes.c_int), ("x_uninf", ctypes.c_int), ("eval", ctypes.c_float),
         ("nohits", ctypes.c_int), ("noalns", ctypes.c_int), ("tc_form", ctypes.c_int),
+        ("autotune", ctypes.c_int),
     ]
 
     @classmethod
@@ -104,6 +105,9 @@ def load_library(path: str | None = None):
         "cbp_format_hits_host": (i32, [vp, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
         "cbp_merge_hit_lists": (i32, [sz, vp, vp, vp, vp]),
         "cbp_write_report": (i32, [vp, vp, vp, vp, sz, vp, sz, ctypes.POINTER(sz)]),
+        "cbp_get_tuning": (i32, [vp, sz, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), vp, i32]),
+        "cbp_set_kernels": (i32, [vp, sz, i32, i32, i32]),
+        "cbp_graph_launches": (i32, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "cbp_db_open": (i32, [ctypes.c_char_p, ctypes.POINTER(vp)]),
         "cbp_db_close": (i32, [vp]),
         "cbp_db_info": (i32, [vp] + [ctypes.POINTER(ctypes.c_uint64)] * 3),
@@ -387,6 +391,27 @@ class BatchProcessing:
         of (annotation, hit record) strings (cbp_format_hits)."""
         from . import report
         return report.format_hits_ctx(self._h, descs, options)
+
+    def tuning(self, query_len: int) -> dict:
+        """The kernel variants in use for this query length and the tuned
+        candidates' sample times (cbp_get_tuning)."""
+        L = load_library()
+        r, w, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = np.zeros(7, np.float32)
+        _check(L.cbp_get_tuning(self._h, int(query_len), ctypes.byref(r), ctypes.byref(w), ctypes.byref(d),
+                                ms.ctypes.data, 7))
+        return {"score_rows": r.value, "order_window": w.value, "dp_warps": d.value,
+                "score_candidates_ms": ms[:5].tolist(), "dp_candidates_ms": ms[5:].tolist()}
+
+    def set_kernels(self, query_len: int, rows: int, window: int, dp_warps: int) -> None:
+        """Fix the kernel variants for this query length (cbp_set_kernels)."""
+        _check(load_library().cbp_set_kernels(self._h, int(query_len), rows, window, dp_warps))
+
+    def graph_launches(self) -> int:
+        """CUDA-graph launches of this context so far (cbp_graph_launches)."""
+        n = ctypes.c_uint64()
+        _check(load_library().cbp_graph_launches(self._h, ctypes.byref(n)))
+        return n.value
 
     def stage_times(self) -> list:
         buf = (ctypes.c_float * 6)()

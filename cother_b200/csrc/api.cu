@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -169,6 +170,24 @@ struct ProfilesStore {
 
 using namespace cbp;
 
+namespace cbp {
+// Kernel variants for one query-length bin: rows per block of the score
+// kernel, the column-ordering window, warps per block of the phase-1 DP;
+// and, once tuned, each candidate's time on the sample.
+constexpr int kScoreCandidates = 5;
+constexpr int kDpCandidates = 2;
+constexpr int kScoreRowsCand[kScoreCandidates] = {16, 8, 32, 16, 16};
+constexpr int kWindowCand[kScoreCandidates] = {1024, 1024, 1024, 256, 4096};
+constexpr int kDpWarpsCand[kDpCandidates] = {2, 1};
+struct Tuning {
+    int rows = 16, window = kOrderWindow, dp_warps = 2;
+    bool tuned = false;
+    float score_ms[kScoreCandidates] = {};
+    float dp_ms[kDpCandidates] = {};
+    long long sample_cols = 0;
+};
+}  // namespace cbp
+
 struct cbp_context {
     int device = 0;
     cbp_options opt{};
@@ -222,6 +241,11 @@ struct cbp_context {
     int last_Lq = 0;
     int last_nprof = 0;
     int last_npass = 0;
+    // kernel variants chosen by the tuner, per query-length bin (Lq / 64)
+    std::map<int, Tuning> tuning;
+    // executable CUDA graph of a slab's phase 1 (plain form)
+    cudaGraphExec_t phase1_exec = nullptr;
+    uint64_t graph_launches = 0;
     // instrumentation
     cudaEvent_t ev[8]{};
     float stage_ms[6] = {0, 0, 0, 0, 0, 0};
@@ -478,6 +502,74 @@ std::vector<Slab> plan_slabs(const cbp_context* c, int Lq)
     return out;
 }
 
+// The tuner: on the first slab of a query-length bin, time each candidate
+// kernel variant on a sample of the slab (its first profiles, up to 32,768
+// positions, all query rows) and keep the fastest. Every variant computes
+// the same cells, so the choice changes the time, never a result; the
+// sample's outputs are overwritten by the slab's own launches.
+void tune_kernels(cbp_context* c, const ScoreArgs& base, int p0, int p1, Tuning& t)
+{
+    const ProfilesStore& db = *c->db;
+    int pe = p0;
+    long long ncols = 0;
+    while (pe < p1 && (pe == p0 || ncols + db.h_plen[pe] <= 32768)) ncols += db.h_plen[pe++];
+    ScoreArgs a = base;
+    a.ncols = (int)ncols;
+    a.ld = align_up(ncols, 32);
+    a.dots_in_scores = false;
+    cudaEvent_t e0 = c->ev[6], e1 = c->ev[7];
+    auto time_it = [&](const std::function<void()>& launch) {
+        float best = 0.f;
+        for (int rep = 0; rep < 2; rep++) {
+            CBP_CUDA(cudaEventRecord(e0, c->stream));
+            launch();
+            CBP_CUDA(cudaEventRecord(e1, c->stream));
+            CBP_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CBP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep == 0 || ms < best) best = ms;
+        }
+        return best;
+    };
+    int bs = 0;
+    for (int k = 0; k < kScoreCandidates; k++) {
+        a.rows = kScoreRowsCand[k];
+        t.score_ms[k] = time_it([&] {
+            launch_column_order(db.view.dstlen, a.col0, a.ncols, a.ld, kWindowCand[k], c->colorder.as<int>(),
+                                c->stream);
+            launch_score_matrix(a, c->stream);
+        });
+        c->launches += 4;
+        if (t.score_ms[k] < t.score_ms[bs]) bs = k;
+    }
+    Dp1Args d;
+    d.scores = a.scores;
+    d.ld = a.ld;
+    d.Lq = a.Lq;
+    d.qtrn = c->query.view.trn;
+    d.db = db.view;
+    d.col0 = a.col0;
+    d.p0 = p0;
+    d.nprof = pe - p0;
+    d.btck = c->btck.as<uint8_t>();
+    d.bandbuf = c->bandbuf.as<float>();
+    d.maxsc = c->dpmax.as<float>();
+    d.maxcoords = c->dpcoords.as<uint32_t>();
+    d.recs = c->dprecs.as<Dp1Rec>();
+    int bd = 0;
+    for (int k = 0; k < kDpCandidates; k++) {
+        d.warps = kDpWarpsCand[k];
+        t.dp_ms[k] = time_it([&] { launch_dp1(d, c->stream); });
+        c->launches += 2;
+        if (t.dp_ms[k] < t.dp_ms[bd]) bd = k;
+    }
+    t.rows = kScoreRowsCand[bs];
+    t.window = kWindowCand[bs];
+    t.dp_warps = kDpWarpsCand[bd];
+    t.sample_cols = ncols;
+    t.tuned = true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -497,6 +589,7 @@ void cbp_default_options(cbp_options* o)
     o->nohits = 700;
     o->noalns = 700;
     o->tc_form = CBP_TC_PLAIN;
+    o->autotune = 1;
 }
 
 const char* cbp_last_error(void) { return g_last_error.c_str(); }
@@ -558,7 +651,8 @@ int cbp_destroy(cbp_context* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->db.reset();
     c->query.release();
-    for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->dpmax, &c->dpcoords,
+    if (c->phase1_exec) cudaGraphExecDestroy(c->phase1_exec);
+    for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->colorder, &c->dpmax, &c->dpcoords,
                       &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
                       &c->cs2, &c->fb2, &c->sg2, &c->bt2, &c->strip2, &c->maperr, &c->alnbuf,
                       &c->cvsmap, &c->statrecs})
@@ -805,9 +899,12 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             a.scores = c->scores.as<float>();
             a.modscores = c->modscores.as<float>();
             a.colorder = c->colorder.as<int>();
-            CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
-            launch_column_order(c->db->view.dstlen, s.col0, s.ncols, a.ld, c->colorder.as<int>(), c->stream);
-            if (c->opt.tc_form != CBP_TC_PLAIN) {
+            Tuning& tn = c->tuning[Lq / 64];
+            if (c->opt.autotune && !tn.tuned) tune_kernels(c, a, s.p0, s.p1, tn);
+            a.rows = tn.rows;
+            const bool tc = c->opt.tc_form != CBP_TC_PLAIN;
+            if (tc) {
+                CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
                 if (!c->cublas) {
                     if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS)
                         throw Error(CBP_ERR_CUDA, "cuBLAS handle creation failed");
@@ -845,15 +942,62 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             d.maxsc = c->dpmax.as<float>();
             d.maxcoords = c->dpcoords.as<uint32_t>();
             d.recs = c->dprecs.as<Dp1Rec>();
+            d.warps = tn.dp_warps;
 
-            launch_score_matrix(a, c->stream);
-            CBP_CUDA(cudaEventRecord(c->ev[1], c->stream));
-            launch_dp1(d, c->stream);
-            CBP_CUDA(cudaEventRecord(c->ev[2], c->stream));
-            launch_dp1_finalize(d, c->score_thld, c->stream);
-            launch_pass_compact(d, c->passidx.as<int>(), c->passdst.as<long long>(), c->passcnt.as<int>(),
-                                reinterpret_cast<long long*>(c->passcnt.as<char>() + 8), c->stream);
-            CBP_CUDA(cudaEventRecord(c->ev[3], c->stream));
+            // phase 1 of the slab: column order, score matrix, DP, its
+            // finalization and the pass list; with the plain form one CUDA
+            // graph, captured here and swapped into the context's executable
+            // graph by an update of its parameters
+            auto phase1 = [&](bool capturing) {
+                auto mark = [&](cudaEvent_t e) {
+                    if (capturing) CBP_CUDA(cudaEventRecordWithFlags(e, c->stream, cudaEventRecordExternal));
+                    else CBP_CUDA(cudaEventRecord(e, c->stream));
+                };
+                if (!tc) mark(c->ev[0]);
+                launch_column_order(c->db->view.dstlen, s.col0, s.ncols, a.ld, tn.window, c->colorder.as<int>(),
+                                    c->stream);
+                launch_score_matrix(a, c->stream);
+                mark(c->ev[1]);
+                launch_dp1(d, c->stream);
+                mark(c->ev[2]);
+                launch_dp1_finalize(d, c->score_thld, c->stream);
+                launch_pass_compact(d, c->passidx.as<int>(), c->passdst.as<long long>(), c->passcnt.as<int>(),
+                                    reinterpret_cast<long long*>(c->passcnt.as<char>() + 8), c->stream);
+                mark(c->ev[3]);
+            };
+            if (tc) {
+                phase1(false);
+            } else {
+                CBP_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                cudaGraph_t g = nullptr;
+                try {
+                    phase1(true);
+                } catch (...) {
+                    cudaStreamEndCapture(c->stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                CBP_CUDA(cudaStreamEndCapture(c->stream, &g));
+                if (c->phase1_exec) {
+                    cudaGraphExecUpdateResultInfo info;
+                    if (cudaGraphExecUpdate(c->phase1_exec, g, &info) != cudaSuccess) {
+                        (void)cudaGetLastError();
+                        cudaGraphExecDestroy(c->phase1_exec);
+                        c->phase1_exec = nullptr;
+                    }
+                }
+                if (!c->phase1_exec) {
+                    const cudaError_t e = cudaGraphInstantiate(&c->phase1_exec, g, 0);
+                    if (e != cudaSuccess) {
+                        cudaGraphDestroy(g);
+                        c->phase1_exec = nullptr;
+                        CBP_CUDA(e);
+                    }
+                }
+                cudaGraphDestroy(g);
+                CBP_CUDA(cudaGraphLaunch(c->phase1_exec, c->stream));
+                c->graph_launches += 1;
+            }
             c->launches += 5;
             c->stage_launches[0] += 2;
             c->stage_launches[1] += 1;
@@ -1205,6 +1349,36 @@ void cbp_score_threshold(size_t query_len, uint64_t db_len, float evalue, float 
     if (log_evalue_threshold) *log_evalue_threshold = lthld;
 }
 
+int cbp_get_tuning(cbp_context* c, size_t query_len, int* rows, int* window, int* dp_warps, float* ms, int n)
+{
+    return guarded([&] {
+        check_ctx(c);
+        const Tuning t = c->tuning.count((int)query_len / 64) ? c->tuning[(int)query_len / 64] : Tuning();
+        if (rows) *rows = t.rows;
+        if (window) *window = t.window;
+        if (dp_warps) *dp_warps = t.dp_warps;
+        for (int k = 0; ms && k < n && k < kScoreCandidates + kDpCandidates; k++)
+            ms[k] = k < kScoreCandidates ? t.score_ms[k] : t.dp_ms[k - kScoreCandidates];
+    });
+}
+
+int cbp_set_kernels(cbp_context* c, size_t query_len, int rows, int window, int dp_warps)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (rows != 8 && rows != 16 && rows != 32) throw Error(CBP_ERR_ARG, "rows per block must be 8, 16 or 32");
+        if (window < 32 || window > kMaxOrderWindow || window % 32)
+            throw Error(CBP_ERR_ARG, "ordering window must be a multiple of 32 in [32, 4096]");
+        if (dp_warps != 1 && dp_warps != 2) throw Error(CBP_ERR_ARG, "DP warps per block must be 1 or 2");
+        Tuning& t = c->tuning[(int)query_len / 64];
+        t = Tuning();
+        t.rows = rows;
+        t.window = window;
+        t.dp_warps = dp_warps;
+        t.tuned = true;
+    });
+}
+
 int cbp_stage_times(cbp_context* c, float* ms, int n)
 {
     if (!c || !ms) return 0;
@@ -1219,6 +1393,14 @@ int cbp_stage_launches(cbp_context* c, uint64_t* launches, int n)
     int k = std::min(n, 6);
     for (int i = 0; i < k; i++) launches[i] = c->stage_launches[i];
     return k;
+}
+
+int cbp_graph_launches(cbp_context* c, uint64_t* graphs)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (graphs) *graphs = c->graph_launches;
+    });
 }
 
 int cbp_launch_count(cbp_context* c, uint64_t* launches)

@@ -13,6 +13,7 @@
 // by shuffle; lane 0 reads the bottom row of the previous band from a
 // per-profile global strip that lane 31 writes. One launch covers every
 // profile of a slab (no per-diagonal launches, no grid-wide syncs).
+#include "cother_b200.h"
 #include "common.cuh"
 #include "cbmath.cuh"
 #include "dp1_kernel.cuh"
@@ -47,7 +48,6 @@ __device__ __forceinline__ bool in_corner(int Lq, int Ld, int edge, int r, int c
 // anti-diagonal reads (lane t reads row t, column s-t: bank (s-t) mod 32);
 // so are the byte tiles of backtrack codes (bank 8*(t mod 4) + a distinct
 // quarter-column per lane).
-constexpr int kDpWarps = 2;             // warps (profiles) per block
 constexpr int kChunk = 32;              // columns per staged chunk
 constexpr int kScoreRing = 3;           // score tiles in flight per warp
 constexpr int kBtckRing = 2;            // backtrack tiles per warp
@@ -114,6 +114,10 @@ __device__ __forceinline__ void store_btck_chunk(const DpStage& st, uint8_t* __r
     for (int i = 0; i < nr; i++) B[(long long)(r0 + i) * ld + c] = tile[i][lane];
 }
 
+// kDpWarps warps (profiles) per block: 1 or 2, chosen by the tuner (each
+// warp stages 18.5 KB of tiles, so a block of 4 would exceed the 48 KB of
+// static shared memory)
+template <int kDpWarps>
 __global__ void __launch_bounds__(32 * kDpWarps)
 dp1_kernel(const Dp1Args a)
 {
@@ -407,8 +411,11 @@ pass_compact_kernel(const Dp1Args a, int* __restrict__ pass_idx, long long* __re
 void launch_dp1(const Dp1Args& a, cudaStream_t stream)
 {
     if (a.nprof <= 0) return;
-    const int blocks = (int)ceil_div(a.nprof, kDpWarps);
-    dp1_kernel<<<blocks, 32 * kDpWarps, 0, stream>>>(a);
+    switch (a.warps) {
+    case 1: dp1_kernel<1><<<(unsigned)a.nprof, 32, 0, stream>>>(a); break;
+    case 2: dp1_kernel<2><<<(unsigned)ceil_div(a.nprof, 2), 64, 0, stream>>>(a); break;
+    default: throw Error(CBP_ERR_ARG, "phase-1 DP warps per block must be 1 or 2");
+    }
     CBP_CHECK_LAUNCH();
 }
 

@@ -31,6 +31,7 @@ struct Dp1Args {
     float* maxsc = nullptr;          // [nprof]
     uint32_t* maxcoords = nullptr;   // [nprof]
     Dp1Rec* recs = nullptr;          // [nprof]
+    int warps = 2;                   // warps (profiles) per block of dp1_kernel: 1 or 2
 };
 
 void launch_dp1(const Dp1Args& a, cudaStream_t stream);

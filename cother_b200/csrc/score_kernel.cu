@@ -15,6 +15,7 @@
 // conflict-free for lanes in step), a 22x22 pair-score table in shared
 // memory, and one code path for upper and lower diagonals.
 #include <cmath>
+#include "cother_b200.h"
 #include "common.cuh"
 #include "cbmath.cuh"
 #include "layout.h"
@@ -27,7 +28,6 @@ namespace {
 constexpr int kCols = 32;          // database positions per block (one per lane)
 constexpr int kWarps = 4;
 constexpr int kThreads = kCols * kWarps;
-constexpr int kRows = 16;          // query positions per block
 constexpr int kElems = 104;        // list elements held per position (99 + overrun)
 constexpr int kDbStride = 108;     // bytes per database list in shared memory (27 words)
 
@@ -238,6 +238,9 @@ __device__ __forceinline__ float cvs_cell(const ScoreArgs& a, const float* __res
     return __ldg(a.cvs_scores + a.cvs_shift + (int)rintf(lo + lo));
 }
 
+// kRows query positions per block (8, 16 or 32; each warp takes every
+// kWarps-th of them), chosen by the tuner
+template <int kRows>
 __global__ void __launch_bounds__(kThreads, 10)
 score_matrix_kernel(const ScoreArgs a)
 {
@@ -444,12 +447,12 @@ score_matrix_kernel(const ScoreArgs a)
 // descending list length (0..kMaxDst). The order within one length is
 // arbitrary: it decides only which lane computes a cell, never its value.
 __global__ void __launch_bounds__(256)
-column_order_kernel(const uint8_t* __restrict__ dstlen, long long col0, int ncols, long long ld,
+column_order_kernel(const uint8_t* __restrict__ dstlen, long long col0, int ncols, long long ld, int window,
                     int* __restrict__ order)
 {
     __shared__ int s_cnt[kMaxDst + 1];
-    const int w0 = blockIdx.x * kOrderWindow;
-    const int n = min(kOrderWindow, ncols - w0);
+    const int w0 = blockIdx.x * window;
+    const int n = min(window, ncols - w0);
     for (int i = threadIdx.x; i <= kMaxDst; i += blockDim.x) s_cnt[i] = 0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x)
@@ -469,28 +472,41 @@ column_order_kernel(const uint8_t* __restrict__ dstlen, long long col0, int ncol
         order[w0 + atomicAdd(&s_cnt[b], 1)] = w0 + i;
     }
     // slots past the last column (the final window only)
-    for (long long i = (long long)w0 + n + threadIdx.x; i < min(ld, (long long)w0 + kOrderWindow);
+    for (long long i = (long long)w0 + n + threadIdx.x; i < min(ld, (long long)w0 + window);
          i += blockDim.x)
         order[i] = -1;
 }
 
-void launch_column_order(const uint8_t* dstlen, long long col0, int ncols, long long ld, int* order,
+void launch_column_order(const uint8_t* dstlen, long long col0, int ncols, long long ld, int window, int* order,
                          cudaStream_t stream)
 {
     if (ncols <= 0) return;
-    column_order_kernel<<<(unsigned)ceil_div(ncols, kOrderWindow), 256, 0, stream>>>(dstlen, col0, ncols, ld,
-                                                                                     order);
+    if (window < 32 || window > kMaxOrderWindow || window % 32)
+        throw Error(CBP_ERR_ARG, "column order window must be a multiple of 32 in [32, 4096]");
+    column_order_kernel<<<(unsigned)ceil_div(ncols, window), 256, 0, stream>>>(dstlen, col0, ncols, ld, window,
+                                                                               order);
+    CBP_CHECK_LAUNCH();
+}
+
+template <int kRows>
+void launch_score_rows(const ScoreArgs& a, cudaStream_t stream)
+{
+    dim3 grid((unsigned)ceil_div(a.ncols, kCols), (unsigned)ceil_div(a.Lq, kRows));
+    const size_t cvs_smem =
+        a.cvswgt > 0.0f ? sizeof(float) * ((kNCV + 2) * kCols + kRows * (kNCV + 1) + 2 * kRows) : 0;
+    score_matrix_kernel<kRows><<<grid, kThreads, cvs_smem, stream>>>(a);
     CBP_CHECK_LAUNCH();
 }
 
 void launch_score_matrix(const ScoreArgs& a, cudaStream_t stream)
 {
     if (a.ncols <= 0 || a.Lq <= 0) return;
-    dim3 grid((unsigned)ceil_div(a.ncols, kCols), (unsigned)ceil_div(a.Lq, kRows));
-    const size_t cvs_smem =
-        a.cvswgt > 0.0f ? sizeof(float) * ((kNCV + 2) * kCols + kRows * (kNCV + 1) + 2 * kRows) : 0;
-    score_matrix_kernel<<<grid, kThreads, cvs_smem, stream>>>(a);
-    CBP_CHECK_LAUNCH();
+    switch (a.rows) {
+    case 8: launch_score_rows<8>(a, stream); break;
+    case 16: launch_score_rows<16>(a, stream); break;
+    case 32: launch_score_rows<32>(a, stream); break;
+    default: throw Error(CBP_ERR_ARG, "score kernel rows per block must be 8, 16 or 32");
+    }
 }
 
 // Pair-score table over packed distance codes (0..20 saturated, 21 = no

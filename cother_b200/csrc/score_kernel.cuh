@@ -13,9 +13,10 @@ struct ScoreArgs {
     int ncols = 0;        // slab positions
     long long ld = 0;     // leading dimension of the outputs
     // slot -> slab column (ld entries, -1 = none): the columns of each
-    // window of kOrderWindow ordered by list length, so that the lanes of a
-    // warp run DDMS loops of equal trip count; nullptr = identity
+    // ordering window sorted by list length, so that the lanes of a warp run
+    // DDMS loops of equal trip count; nullptr = identity
     const int* colorder = nullptr;
+    int rows = 16;        // query positions per block: 8, 16 or 32
     int Lq = 0;
     float ssswgt = 0.f, ddmswgt = 0.f, initshift = 0.f;
     int dstsegm = 6;
@@ -36,14 +37,16 @@ struct ScoreArgs {
     bool dots_in_scores = false;
 };
 
-// columns per ordering window of launch_column_order
+// columns per ordering window of launch_column_order: default and largest
 constexpr int kOrderWindow = 1024;
+constexpr int kMaxOrderWindow = 4096;
 
 void launch_score_matrix(const ScoreArgs& a, cudaStream_t stream);
 // Fill order[0..ld) for the slab columns [col0, col0+ncols): within each
-// window of kOrderWindow slots, the window's columns by descending distance
-// list length; slots past ncols get -1.
-void launch_column_order(const uint8_t* dstlen, long long col0, int ncols, long long ld, int* order,
+// window of `window` slots (a multiple of 32, at most kMaxOrderWindow), the
+// window's columns by descending distance list length; slots past ncols
+// get -1.
+void launch_column_order(const uint8_t* dstlen, long long col0, int ncols, long long ld, int window, int* order,
                          cudaStream_t stream);
 void build_dms_table(float* T);
 

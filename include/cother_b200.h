@@ -77,11 +77,17 @@ typedef struct cbp_options {
                        * which sums the 20 quotients on CUDA cores); results agree
                        * with the plain form within about 1e-6 relative, not bit
                        * for bit. */
+    int   autotune;   /* 1: on the first slab of each query-length bin (Lq/64), time
+                       * the kernel variants (score-kernel rows per block and
+                       * column-ordering window, phase-1 DP warps per block) on a
+                       * sample of the slab and keep the fastest (no counterpart in
+                       * the reference). Results do not depend on the choice. */
 } cbp_options;
 
 /* Fill *opt with the values of the parity configuration:
  * SSSWGT=0.12, CVSWGT=0, DDMSWGT=0.2, DSTSEGM=6, MAPALN=1, MINPP=0.28,
- * SSEMODEL=2, X_UNINF=1, EVAL=10, NOHITS=NOALNS=700. */
+ * SSEMODEL=2, X_UNINF=1, EVAL=10, NOHITS=NOALNS=700; the plain FP32
+ * profile-profile form and the kernel tuner on. */
 void cbp_default_options(cbp_options* opt);
 
 /* Create a context on `device`.
@@ -435,6 +441,19 @@ int cbp_dp1_noalloc(const float* scores, size_t ld, int query_len, const float* 
  * the memory budget). Used to exercise multi-slab processing. */
 int cbp_set_max_slab_positions(cbp_context* ctx, size_t max_positions);
 
+/* The kernel variants in use for queries of length query_len (the tuner's
+ * choice for its bin, or the defaults 16 / 1024 / 2 before tuning or with
+ * autotune = 0): score-kernel query rows per block, column-ordering window,
+ * phase-1 DP warps per block; and in ms[0..n) the tuned candidates' times on
+ * the sample (score variants (16,1024), (8,1024), (32,1024), (16,256),
+ * (16,4096), then DP variants 2 and 1 warps). */
+int cbp_get_tuning(cbp_context* ctx, size_t query_len, int* rows, int* window, int* dp_warps,
+                   float* ms, int n);
+
+/* Fix the kernel variants for queries in query_len's bin (no tuning
+ * there): rows 8/16/32, window a multiple of 32 up to 4096, dp_warps 1/2. */
+int cbp_set_kernels(cbp_context* ctx, size_t query_len, int rows, int window, int dp_warps);
+
 /* Device time in milliseconds of the kernels of the last cbp_process()
  * call, per stage: [0] score matrix, [1] phase-1 DP, [2] phase-1
  * finalization, [3] statistics, [4] MAP phase, [5] result assembly.
@@ -444,6 +463,13 @@ int cbp_stage_times(cbp_context* ctx, float* ms, int n);
 /* Kernel launches of the last cbp_process() call per stage (same stage
  * order as cbp_stage_times). Returns the number of stages written. */
 int cbp_stage_launches(cbp_context* ctx, uint64_t* launches, int n);
+
+/* Number of CUDA-graph launches since the context was created: with the
+ * plain form each slab's phase 1 (column order, score matrix, DP,
+ * finalization, pass list) runs as one executable graph, captured on the
+ * slab's parameters and updated in place (no counterpart in the
+ * reference, which launches once per block diagonal from the host). */
+int cbp_graph_launches(cbp_context* ctx, uint64_t* graphs);
 
 /* Number of kernel launches issued by the last cbp_process() call. */
 int cbp_launch_count(cbp_context* ctx, uint64_t* launches);
