@@ -390,7 +390,8 @@ def main():
                     recs[order[:50], 1].view(np.uint32).tobytes()).hexdigest()[:16],
                 "merged_hits": merged_hits if world > 1 else None,
                 "stage_ms": {k: v / steps for k, v in zip(STAGES, stage_acc)},
-                "gpu_launches": launches, "roofline": roof, "clocks": clocks}
+                "gpu_launches": launches, "graph_launches": bp.graph_launches(),
+                "tuning": bp.tuning(Lq), "roofline": roof, "clocks": clocks}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds, db_len, nseqs, args.cvswgt)
         print(json.dumps(line))
