@@ -76,3 +76,51 @@ def test_forms_report_the_same_top_hits(ss_table):
         assert np.array_equal(p1, p0), form
         assert np.all(np.abs(s1 - s0) <= 1e-4 * np.abs(s0) + 1e-6), form
         assert np.all(np.abs(e1 - e0) <= 1e-3 * np.abs(e0) + 1e-6), form
+
+
+def test_forms_dp_optima_and_evalues_against_fp64(ss_table):
+    """Phase-1 optima and log E-values of each form against the same stages
+    run by the oracle on FP64 cell scores (the profile-profile term alone,
+    rounded once to FP32): the DP and the statistics stay FP32 in every
+    form, so this isolates the error the contraction brings into them."""
+    import cother_b200 as cb
+    from cother_b200 import synth
+    from oracle import oracle as O
+    q = synth.make_profiles([150], 971, True)
+    db = synth.make_profiles(synth.lognormal_lengths(40, 150, 30, 400, seed=972), 973, False)
+    synth.plant_homologs(q, db, 0.2, seed=974)
+    qtf = q.tf.astype(np.float64)
+    qbg = q.bkg[:, 0].astype(np.float64)
+    dbg = db.bkg.astype(np.float64)[:, db.addrpro]
+    ref = (np.log(qtf.T @ (db.tf.astype(np.float64) / (0.5 * (qbg[:, None] + dbg)))) - 0.002)
+    ref32 = ref.astype(np.float32)
+    thld = -1.0e30
+    rec64, _ = O.dp1(q, db, ref32, 0, 0, db.nprofiles, thld)
+    sspace = float(db.npositions) * q.npositions
+
+    def logE(S, rec):
+        out = []
+        for p in range(db.nprofiles):
+            s0, Ld = int(db.starts[p]), int(db.lens[p])
+            st, _ = O.pair_statistics(S[:, s0:s0 + Ld], q.aa, db.aa[s0:s0 + Ld], rec["score"][p],
+                                      rec["psts"][p], q.npositions, Ld, q.eno[0], db.eno[p], sspace)
+            out.append(st[2])
+        return np.array(out, np.float64)
+
+    e64 = logE(ref32, rec64)
+    report = {}
+    for name, form in (("plain", cb.TC_PLAIN), ("bf16x3", cb.TC_BF16X3), ("tf32x3", cb.TC_TF32X3)):
+        sc = _scores(q, db, ss_table, ssswgt=0.0, ddmswgt=0.0, tc_form=form).astype(np.float32)
+        rec, _ = O.dp1(q, db, sc, 0, 0, db.nprofiles, thld)
+        e = logE(sc, rec)
+        d_cell = float(np.max(np.abs(sc.astype(np.float64) - ref)))
+        d_opt = float(np.max(np.abs(rec["maxsc"].astype(np.float64) - rec64["maxsc"]) /
+                             np.maximum(np.abs(rec64["maxsc"].astype(np.float64)), 1.0)))
+        d_sc = float(np.max(np.abs(rec["score"].astype(np.float64) - rec64["score"]) /
+                            np.maximum(np.abs(rec64["score"].astype(np.float64)), 1.0)))
+        d_e = float(np.max(np.abs(e - e64) / np.maximum(np.abs(e64), 1.0)))
+        report[name] = (d_cell, d_opt, d_sc, d_e)
+        assert d_opt < 1e-4 and d_sc < 1e-4 and d_e < 1e-3, (name, report[name])
+    print("\nform    cell max-abs  DP optimum rel  phase-1 score rel  log E rel   (vs FP64 cells)")
+    for name, (a, b, c, d) in report.items():
+        print(f"{name:7s} {a:12.3e}  {b:14.3e}  {c:17.3e}  {d:10.3e}")
