@@ -112,7 +112,9 @@ constexpr float kTiny = 0x1p-149f;
 
 // One diagonal of the DDMS segment DP. Elements e = 0,1,... pair query list
 // element oq+e with database list element od+e (upper diagonals: oq = 0,
-// od = j; lower: oq = i, od = 0). Pair scores at even offsets within each
+// od = j; lower: oq = i, od = 0). The lists hold their codes pre-multiplied
+// into byte offsets of the pair-score table T (query: code x 88, a row of
+// 22 floats; database: code x 4), so a pair score is one add and one load. Pair scores at even offsets within each
 // 4-step are table values, odd ones the mean of their neighbours
 // (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:184-198); a segment
 // restarts when the running sum has fallen to zero, and the best segment of
@@ -130,18 +132,18 @@ constexpr float kTiny = 0x1p-149f;
 // attains it, which is the reference's strict "<" scan. `thr` is
 // max(third entry's score, kTiny): a candidate below it changes nothing.
 __device__ __forceinline__ void ddms_diagonal(
-    const uint8_t* __restrict__ q, const uint8_t* __restrict__ d,
-    const float* __restrict__ T, int lim, int oq, int od, float nsegm1,
+    const uint16_t* __restrict__ q, const uint8_t* __restrict__ d,
+    const char* __restrict__ T, int lim, int oq, int od, float nsegm1,
     float (&ms)[3], uint32_t (&mb)[3], uint32_t (&me)[3], float& thr)
 {
     constexpr float kBig = 0x1p100f;
-    float s0 = T[q[0] * kDstCard + d[0]];
+    float s0 = *reinterpret_cast<const float*>(T + q[0] + d[0]);
     float t = sat_add(s0, 0.0f);
     float ls = 1.0f;
     const uint32_t cbase = ((uint32_t)oq << 16) | (uint32_t)od;
     for (int x = 0; x < lim; x += 4) {
-        const float s2 = T[q[x + 2] * kDstCard + d[x + 2]];
-        const float s4 = T[q[x + 4] * kDstCard + d[x + 4]];
+        const float s2 = *reinterpret_cast<const float*>(T + q[x + 2] + d[x + 2]);
+        const float s4 = *reinterpret_cast<const float*>(T + q[x + 4] + d[x + 4]);
         const float l1 = __fmaf_rn(ls, sat_mul(t, kBig), 1.0f);
         const float t1 = sat_fma(0.5f, s0 + s2, t);
         const float l2 = __fmaf_rn(l1, sat_mul(t1, kBig), 1.0f);
@@ -188,9 +190,9 @@ __device__ __forceinline__ void ddms_diagonal(
 
 // DDMS of one cell (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s_h2.cuh:433-500).
 // Returns the top-3 sum in the reference's scale.
-__device__ __forceinline__ float ddms_cell(const uint8_t* __restrict__ q, int len1,
+__device__ __forceinline__ float ddms_cell(const uint16_t* __restrict__ q, int len1,
                                            const uint8_t* __restrict__ d, int len2,
-                                           const float* __restrict__ T, int dstsegm)
+                                           const char* __restrict__ T, int dstsegm)
 {
     float ms[3] = {0.0f, 0.0f, 0.0f};
     uint32_t mb[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
@@ -247,7 +249,7 @@ score_matrix_kernel(const ScoreArgs a)
     __shared__ float s_dms[kDstCard * kDstCard];
     __shared__ float s_sst[kSSCard * kSSCard];
     __shared__ __align__(16) uint8_t s_dbe[kCols * kDbStride];
-    __shared__ __align__(16) uint8_t s_qe[kRows * kElems];
+    __shared__ __align__(16) uint16_t s_qe[kRows * kElems];
     __shared__ float s_dtf[kNAA][kCols];
     __shared__ float s_dbg[kNAA][kCols];
     __shared__ float s_dss[kNSS][kCols];
@@ -296,7 +298,9 @@ score_matrix_kernel(const ScoreArgs a)
     } else if (warp == kNSS) {
         s_dlen[lane] = 0;
     }
-    // distance lists: 32 columns x 104 bytes, in 16-byte pieces
+    // distance lists: 32 columns x 104 bytes, in 16-byte pieces, each code
+    // times 4 (a byte offset in a row of the pair-score table; codes <= 21,
+    // so the shift never carries across bytes)
     for (int idx = tid; idx < kCols * 7; idx += kThreads) {
         const int c = idx / 7, piece = idx - c * 7;
         const int cc = s_col[c];
@@ -308,8 +312,8 @@ score_matrix_kernel(const ScoreArgs a)
             v = make_uint4(f, f, f, f);
         }
         uint32_t* dstw = reinterpret_cast<uint32_t*>(s_dbe + c * kDbStride + piece * 16);
-        dstw[0] = v.x; dstw[1] = v.y; dstw[2] = v.z;
-        if (piece < 6) dstw[3] = v.w;   // piece 6 covers bytes 96..107 only
+        dstw[0] = v.x << 2; dstw[1] = v.y << 2; dstw[2] = v.z << 2;
+        if (piece < 6) dstw[3] = v.w << 2;   // piece 6 covers bytes 96..107 only
     }
     // query rows of this block
     for (int idx = tid; idx < kRows * kNAA; idx += kThreads) {
@@ -343,12 +347,17 @@ score_matrix_kernel(const ScoreArgs a)
     }
     if (tid < kNAA) s_qbg[tid] = a.q.bkg[tid];
     if (tid < kRows) s_qlen[tid] = (rowb + tid < a.Lq) ? a.q.dstlen[rowb + tid] : 0;
+    // query lists: each code times 88, the byte offset of its table row
     for (int idx = tid; idx < kRows * (kElems / 4); idx += kThreads) {
         const int r = idx / (kElems / 4), w = idx - r * (kElems / 4);
         const int row = rowb + r;
         uint32_t v = 0x15151515u;
         if (row < a.Lq) v = *reinterpret_cast<const uint32_t*>(a.q.dst + (long long)row * kDstStride + 4 * w);
-        reinterpret_cast<uint32_t*>(s_qe + r * kElems)[w] = v;
+        uint16_t* o = s_qe + r * kElems + 4 * w;
+        o[0] = (uint16_t)((v & 0xffu) * (kDstCard * 4));
+        o[1] = (uint16_t)(((v >> 8) & 0xffu) * (kDstCard * 4));
+        o[2] = (uint16_t)(((v >> 16) & 0xffu) * (kDstCard * 4));
+        o[3] = (uint16_t)((v >> 24) * (kDstCard * 4));
     }
     __syncthreads();
 
@@ -425,7 +434,8 @@ score_matrix_kernel(const ScoreArgs a)
         if (a.ddmswgt > 0.0f) {
             const int qlen = s_qlen[r];
             if (qlen >= a.dstsegm && dlen >= a.dstsegm) {
-                const float sum = ddms_cell(s_qe + r * kElems, qlen, de, dlen, s_dms, a.dstsegm);
+                const float sum = ddms_cell(s_qe + r * kElems, qlen, de, dlen,
+                                            reinterpret_cast<const char*>(s_dms), a.dstsegm);
                 const float dm = __fmaf_rn(0.053f * 16.0f, sum, -1.235f) * a.ddmswgt;
                 if (dm != 0.0f) {
                     // the modular score drops 0.2*DDMSWGT, in the contracted
