@@ -34,10 +34,10 @@ sys.path.insert(0, ROOT)
 
 DEFAULT_WORKLOAD = "q400_db50k"
 # DRAM bytes (read + write) per cell of one score_matrix_kernel launch,
-# measured by ncu on q400 x 2,000 profiles (4.32 GB for 195.0 M cells:
-# 8 B/cell of score writes plus the database lists re-read by each 16-row
-# block); the traffic grows with the cells
-SCORE_DRAM_BYTES_PER_CELL = 22.16
+# measured by ncu on q400 x 2,000 profiles (3.03 GB for 195.0 M cells with
+# the 32-row variant: 8 B/cell of score writes plus the database lists
+# re-read by each block of query rows); the traffic grows with the cells
+SCORE_DRAM_BYTES_PER_CELL = 15.51
 STAGES = ["score_matrix", "phase1_dp", "phase1_finalize", "statistics", "map_realignment"]
 OPS_PER_DDMS_STEP = 50  # algorithmic ops of one 4-cell DDMS step (2 pair scores,
                         # 2 interpolations, 4 segment updates, 1 top-3 register)
