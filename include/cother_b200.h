@@ -145,9 +145,11 @@ int cbp_db_info(cbp_db* db, uint64_t* nprofiles, uint64_t* npositions, uint64_t*
 int cbp_db_profile_lengths(cbp_db* db, int32_t* lens);
 /* Profiles first .. first+count-1 as the 181 begin/end field pointers that
  * cbp_transfer_chunk takes, and their descriptions (descs may be NULL; else
- * count entries). The stored fields point into the mapped file; the derived
- * ones (pps2DDist, pmv2DAddrPro, pmv2DAddrCV, pmv2DAddrSS) into buffers of
- * the handle. Valid until the next cbp_db_chunk call or cbp_db_close. */
+ * count entries). The stored fields point into the mapped file, which is
+ * mapped read-only (the pointers are char* only to match cbp_transfer_chunk,
+ * which never writes through them); the derived ones (pps2DDist,
+ * pmv2DAddrPro, pmv2DAddrCV, pmv2DAddrSS) into buffers of the handle. Valid
+ * until the next cbp_db_chunk call or cbp_db_close. */
 int cbp_db_chunk(cbp_db* db, uint64_t first, uint64_t count, char** beg, char** end,
                  const char** descs);
 /* Write profiles given as a 181-field table (one chunk: all fields of the
