@@ -38,6 +38,15 @@ DEFAULT_WORKLOAD = "q400_db50k"
 # the 32-row variant: 8 B/cell of score writes plus the database lists
 # re-read by each block of query rows); the traffic grows with the cells
 SCORE_DRAM_BYTES_PER_CELL = 15.51
+
+
+def score_traffic_per_cell(rows: int) -> float:
+    """DRAM bytes per cell of the score kernel with `rows` query rows per
+    block: the 8 B/cell of score writes plus the database reads, which each
+    block of rows repeats (measured at 32 rows)."""
+    return 8.0 + (SCORE_DRAM_BYTES_PER_CELL - 8.0) * 32.0 / rows
+
+
 STAGES = ["score_matrix", "phase1_dp", "phase1_finalize", "statistics", "map_realignment"]
 OPS_PER_DDMS_STEP = 50  # algorithmic ops of one 4-cell DDMS step (2 pair scores,
                         # 2 interpolations, 4 segment updates, 1 top-3 register)
@@ -357,6 +366,7 @@ def main():
 
     if rank == 0:
         peaks = measured_peaks()
+        rows = bp.tuning(Lq)["score_rows"]
         score_launch_ms = score_ms / max(1, score_launches)
         # one launch per slab; the workload here fits one slab
         ops = steps_ddms * OPS_PER_DDMS_STEP * args.steps / max(1, score_launches)
@@ -365,10 +375,12 @@ def main():
         alu_peak = 148 * 128 * sm_mhz * 1e6 / 1e9  # lane-ops/s at max clock, Gop/s
         roof = {"bound": "alu", "achieved": achieved, "peak": alu_peak, "unit": "Gop/s",
                 "frac": achieved / alu_peak,
-                "traffic": SCORE_DRAM_BYTES_PER_CELL * float(Lq) * Ndb,
+                "traffic": score_traffic_per_cell(rows) * float(Lq) * Ndb,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                  "score_matrix_kernel launch at q400 x 2,000 profiles, "
-                                  "scaled by cells (profiles/score_matrix_kernel_q400_db2k.md)",
+                                  "score_matrix_kernel launch at q400 x 2,000 profiles with 32 "
+                                  "rows per block, scaled by cells and, for the %d-row variant "
+                                  "in use, by the database reads per block "
+                                  "(profiles/score_matrix_kernel_q400_db2k.md)" % rows,
                 "kernel": "score_matrix_kernel",
                 "peak_source": "148 SMs x 128 FP32 lanes x max SM clock (nominal issue rate)",
                 "hbm_bytes_per_launch": float(Lq) * Ndb * 8,
