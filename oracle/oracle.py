@@ -23,7 +23,8 @@ _ref = None
 
 def build(force: bool = False) -> None:
     """Compile the oracle and, when the reference tree is present, the
-    reference's DDMS restatement and its CUDA kernels (oracle/_ref/)."""
+    reference's DDMS restatement, its CUDA kernels and its description
+    formatters (oracle/_ref/)."""
     args = ["make", "-s", "-C", HERE, "all"]
     if force:
         subprocess.run(["make", "-s", "-C", HERE, "clean"], check=True)
@@ -32,6 +33,8 @@ def build(force: bool = False) -> None:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
     if os.path.isdir(os.path.join(REFERENCE_TREE, "src", "libmycu")):
         subprocess.run(["make", "-s", "-C", HERE, "refgpu"], check=True)
+    if os.path.isfile(os.path.join(REFERENCE_TREE, "src", "liblib", "fmtdescription.h")):
+        subprocess.run(["make", "-s", "-C", HERE, "fmtref"], check=True)
 
 
 def lib():
