@@ -163,17 +163,18 @@ def measured_peaks():
         return None
 
 
-def oracle_pipeline(q, db, ss, nprof, nthreads, db_len, nseqs, cvswgt=0.0):
+def oracle_pipeline(q, db, ss, nthreads, db_len, nseqs, cvswgt=0.0):
     """The oracle's whole search path (score matrix, phase 1, statistics,
-    MAP realignment) for the query against the first `nprof` profiles."""
+    MAP realignment) for the query against the profile set `db` (a sample
+    of the workload's database); E-values for a database of `db_len`
+    positions and `nseqs` profiles. Loads the oracle only, never the
+    product library."""
     from oracle import oracle as O
-    import cother_b200 as cb
-    db = db.subset(0, nprof)
     ncols = db.npositions
     sc, ms = O.score_matrix(q, db, ss, ncols=ncols, nthreads=nthreads, cvswgt=cvswgt)
-    thld, lthld = cb.score_threshold(q.npositions, db_len)
+    thld, lthld = O.score_threshold(q.npositions, db_len)
     sspace, _ = O.length_adjustment(q.npositions, db_len, nseqs)
-    rec, _ = O.dp1(q, db, sc, 0, 0, nprof, thld)
+    rec, _ = O.dp1(q, db, sc, 0, 0, db.nprofiles, thld)
     for p in np.nonzero(rec["passed"])[0]:
         s0, Ld = int(db.starts[p]), int(db.lens[p])
         st, _ = O.pair_statistics(sc[:, s0:s0 + Ld], q.aa, db.aa[s0:s0 + Ld], rec["score"][p],
@@ -183,55 +184,120 @@ def oracle_pipeline(q, db, ss, nprof, nthreads, db_len, nseqs, cvswgt=0.0):
     return ncols
 
 
+def spread_sample(db, nprof: int) -> np.ndarray:
+    """`nprof` profile indices spread evenly over the whole database."""
+    nprof = int(max(1, min(db.nprofiles, nprof)))
+    return np.unique(np.linspace(0, db.nprofiles - 1, nprof).round().astype(np.int64))
+
+
+class CpuTimer:
+    """The oracle pipeline on the host cores over bounded samples of the
+    workload's database (profiles spread across it), calibrated so that a
+    sample takes about the requested seconds."""
+
+    def __init__(self, q, db, ss, db_len, nseqs, cvswgt=0.0):
+        self.q, self.db, self.ss = q, db, ss
+        self.db_len, self.nseqs, self.cvswgt = db_len, nseqs, cvswgt
+        self.rate = {}
+
+    def _run(self, idx, nthreads):
+        sub = self.db.select(idx)
+        t = time.perf_counter()
+        cols = oracle_pipeline(self.q, sub, self.ss, nthreads, self.db_len, self.nseqs, self.cvswgt)
+        return cols, max(time.perf_counter() - t, 1e-6)
+
+    def measure(self, seconds: float, nthreads: int):
+        if nthreads not in self.rate:
+            cols, dt = self._run(spread_sample(self.db, 4), nthreads)
+            self.rate[nthreads] = cols / dt
+        mean_len = float(self.db.lens.mean())
+        idx = spread_sample(self.db, max(4, self.rate[nthreads] * seconds / mean_len))
+        cols, dt = self._run(idx, nthreads)
+        cells = self.q.npositions * cols
+        return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": nthreads,
+                "kind": "port",
+                "sample": f"query {self.q.npositions} x {len(idx)} database profiles spread over "
+                          f"all {self.db.nprofiles} ({cols} positions, {cells} cells, {dt:.1f} s), "
+                          f"whole path (score matrix on {nthreads} threads, phase 1, statistics, "
+                          f"MAP); E-values for the whole database"}
+
+
 def cpu_baseline(q, db, ss, seconds: float, db_len: int, nseqs: int, cvswgt: float = 0.0):
-    """Oracle (a port of the reference kernels) on the host cores, on a
-    bounded sample: the query against the first database profiles, through
-    the whole path."""
+    """The oracle (a port of the reference's kernels; the reference has no
+    CPU path) on all host cores and on one core, each on a bounded sample
+    of the same workload."""
     ncpu = os.cpu_count() or 1
-    # calibrate on a few profiles, then size the timed sample
-    probe = min(db.nprofiles, 4)
-    t = time.perf_counter()
-    cols = oracle_pipeline(q, db, ss, probe, ncpu, db_len, nseqs, cvswgt)
-    dt = max(time.perf_counter() - t, 1e-3)
-    rate = cols / dt
-    mean_len = float(db.lens.mean())
-    nprof = int(min(db.nprofiles, max(probe, rate * seconds / mean_len)))
-    t = time.perf_counter()
-    cols = oracle_pipeline(q, db, ss, nprof, ncpu, db_len, nseqs, cvswgt)
-    dt = time.perf_counter() - t
-    cells = q.npositions * cols
-    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": ncpu, "kind": "port",
-            "sample": f"query {q.npositions} x first {nprof} database profiles ({cols} positions, "
-                      f"{cells} cells, {dt:.1f} s), whole path (score matrix, phase 1, "
-                      f"statistics, MAP), score matrix on {ncpu} threads"}
+    timer = CpuTimer(q, db, ss, db_len, nseqs, cvswgt)
+    out = timer.measure(seconds * 0.6, ncpu)
+    out["single_thread"] = timer.measure(seconds * 0.4, 1)
+    return out
+
+
+def workload_config(args, q, db, world: int) -> dict:
+    """The `config` of the JSON line: the same for both arms."""
+    return {"workload": args.workload, "query_len": q.npositions, "db_profiles": db.nprofiles,
+            "db_positions": db.npositions, "stages": STAGES, "tc_form": args.tc,
+            "cvswgt": args.cvswgt, "l2": "inputs larger than L2 (database chunk > 126 MB)",
+            "parallelism": f"dp{world} (database shard per GPU)"}
+
+
+def reference_gpu_kernels(args):
+    """Device time of the reference's own CUDA kernels (compiled from its
+    sources for sm_100a into oracle/_ref) on the same workload, or None when
+    they are not built. Runs after the CPU arm's timed steps."""
+    lib = os.path.join(ROOT, "oracle", "_ref", "librefgpu.so")
+    if not os.path.exists(lib) or args.tc != "plain" or args.cvswgt > 0:
+        return None
+    cmd = [sys.executable, os.path.join(ROOT, "oracle", "time_ref_gpu.py"), "--workload",
+           args.workload, "--seed", str(args.seed), "--repeats", "2"]
+    if args.ndb:
+        cmd += ["--ndb", str(args.ndb)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode != 0 or not line:
+            return {"unavailable": (r.stderr.strip().splitlines() or ["no output"])[-1][:300]}
+        d = json.loads(line[-1])
+        return {"value": d["gcups"], "unit": "GCUPS", "stage_ms": d["stage_ms"],
+                "total_ms": d["total_ms"], "chunks": d["chunks"],
+                "what": "the reference's own score-matrix, phase-1, statistics and MAP kernels, "
+                        "compiled from its sources for sm_100a, same workload and query, device "
+                        "time (oracle/time_ref_gpu.py)"}
+    except Exception as e:  # a measurement beside the arm's value, never its result
+        return {"unavailable": str(e)[:300]}
 
 
 def run_reference(args):
     """--impl reference: the oracle port of the reference's kernels on the
-    host cores (the reference has no CPU path of its own)."""
+    host cores (the reference has no CPU path of its own), on the same
+    workload as the product arm: the full database is generated and each
+    step searches the query against a bounded sample of it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from cother_b200 import synth
     ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
-    ndb = args.ndb or 200
-    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=ndb, qindex=args.qindex,
+    q, db = synth.make_workload(args.workload, seed=args.seed, ndb=args.ndb, qindex=args.qindex,
                                 context_vectors=args.cvswgt > 0)
-    vals = []
-    full = synth.db_lengths(args.workload, args.seed)
-    db_len, nseqs = int(full.sum()), len(full)
-    for _ in range(max(1, args.warmup) + args.steps):
-        vals.append(cpu_baseline(q, db, ss, args.cpu_seconds / 3, db_len, nseqs, args.cvswgt))
+    db_len, nseqs = db.npositions, db.nprofiles
+    ncpu = os.cpu_count() or 1
+    timer = CpuTimer(q, db, ss, db_len, nseqs, args.cvswgt)
+    per_step = max(1.0, args.cpu_seconds / 3)
+    vals = [timer.measure(per_step, ncpu) for _ in range(max(3, args.warmup) + args.steps)]
     timed = vals[-args.steps:] if args.steps > 0 else vals
     v = float(np.mean([x["value"] for x in timed]))
     cb = dict(timed[-1])
     cb["value"] = v
+    cb["single_thread"] = timer.measure(per_step, 1)
     line = {"impl": "reference", "metric": "GCUPS", "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "stages": STAGES, "cvswgt": args.cvswgt},
+            "config": workload_config(args, q, db, args.gpus),
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    ref_gpu = reference_gpu_kernels(args)
+    if ref_gpu is not None:
+        line["reference_gpu_kernels"] = ref_gpu
     print(json.dumps(line))
 
 
@@ -389,11 +455,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern_ms / steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
-                "config": {"workload": args.workload, "query_len": Lq, "db_profiles": db.nprofiles,
-                           "db_positions": Ndb, "stages": STAGES, "tc_form": args.tc,
-                           "cvswgt": args.cvswgt,
-                           "l2": "inputs larger than L2 (database chunk > 126 MB)",
-                           "parallelism": f"dp{world} (database shard per GPU)"},
+                "config": workload_config(args, q, db, world),
                 "e2e": {"value": e2e, "unit": "GCUPS",
                         "h2d_bytes_per_step": int(Lq * (4 * 20 + 4 * 3 + 4 * 100 + 2) + 4 * 7 * (Lq + 1)),
                         "d2h_bytes_per_step": int(d2h)},

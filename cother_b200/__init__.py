@@ -85,6 +85,7 @@ def load_library(path: str | None = None):
         "cbp_read_phase1": (i32, [vp, vp, vp, vp, vp, vp, sz, ctypes.POINTER(sz), vp,
                                   ctypes.POINTER(sz)]),
         "cbp_read_btck": (i32, [vp, vp, sz]),
+        "cbp_read_slab_columns": (i32, [vp, sz, sz, vp, vp, vp, sz]),
         "cbp_score_threshold": (None, [sz, ctypes.c_uint64, f32, f32, f32, ctypes.POINTER(f32),
                                        ctypes.POINTER(f32)]),
         "cbp_get_hit_records": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
@@ -385,6 +386,16 @@ class BatchProcessing:
         b = np.zeros((nrows, max_cols), np.uint8)
         _check(load_library().cbp_read_btck(self._h, b.ctypes.data, max_cols))
         return b
+
+    def read_slab_columns(self, nrows: int, first_col: int, ncols: int):
+        """(scores, modscores, btck) of slab columns [first_col,
+        first_col + ncols) of the last slab (cbp_read_slab_columns)."""
+        sc = np.zeros((nrows, max(ncols, 1)), np.float32)
+        ms = np.zeros((nrows, max(ncols, 1)), np.float32)
+        bt = np.zeros((nrows, max(ncols, 1)), np.uint8)
+        _check(load_library().cbp_read_slab_columns(self._h, int(first_col), int(ncols), sc.ctypes.data,
+                                                     ms.ctypes.data, bt.ctypes.data, sc.shape[1]))
+        return sc[:, :ncols], ms[:, :ncols], bt[:, :ncols]
 
     def format_hits(self, descs=None, options=None):
         """Per-hit text of the last search in the finalizer's order: a list

@@ -1234,6 +1234,30 @@ int cbp_read_btck(cbp_context* c, uint8_t* btck, size_t ld)
     });
 }
 
+int cbp_read_slab_columns(cbp_context* c, size_t first_col, size_t ncols, float* scores, float* modscores,
+                          uint8_t* btck, size_t ld)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!c->last_Lq) throw Error(CBP_ERR_STATE, "no processed query");
+        if (first_col > (size_t)c->last_ncols || ncols > (size_t)c->last_ncols - first_col)
+            throw Error(CBP_ERR_ARG, "column range outside the slab");
+        if (ld < ncols) throw Error(CBP_ERR_ARG, "ld smaller than the column count");
+        if (ncols == 0) return;
+        CBP_CUDA(cudaStreamSynchronize(c->stream));
+        const size_t w = ncols * sizeof(float);
+        if (scores)
+            CBP_CUDA(cudaMemcpy2D(scores, ld * sizeof(float), (const float*)c->scores.p + first_col,
+                                  c->last_ld * sizeof(float), w, c->last_Lq, cudaMemcpyDeviceToHost));
+        if (modscores)
+            CBP_CUDA(cudaMemcpy2D(modscores, ld * sizeof(float), (const float*)c->modscores.p + first_col,
+                                  c->last_ld * sizeof(float), w, c->last_Lq, cudaMemcpyDeviceToHost));
+        if (btck)
+            CBP_CUDA(cudaMemcpy2D(btck, ld, (const uint8_t*)c->btck.p + first_col, c->last_ld, ncols,
+                                  c->last_Lq, cudaMemcpyDeviceToHost));
+    });
+}
+
 int cbp_get_hit_records(cbp_context* c, float* recs, size_t max_records, size_t* nrecords)
 {
     return guarded([&] {

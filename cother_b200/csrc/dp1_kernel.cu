@@ -129,6 +129,16 @@ dp1_kernel(const Dp1Args a)
     const int p = a.p0 + pl;
     const int Ld = a.db.plen[p];
     const long long colb = a.db.pstart[p] - a.col0;
+    if (colb < 0 || colb + Ld > a.ld || Ld >= 65536) {
+        // a profile outside the slab's columns (or too long for the 16-bit
+        // cell coordinates) is skipped: nothing of it is read or written,
+        // and its maximum is flagged as NaN with coordinates 0xffffffff
+        if (lane == 0) {
+            a.maxsc[pl] = __int_as_float(0x7fc00000);
+            a.maxcoords[pl] = 0xffffffffu;
+        }
+        return;
+    }
     const long long tb = a.db.pstart[p] + p;        // beginning-transition entry
     const long long NT = a.db.N + a.db.P;
     const int Lq = a.Lq;

@@ -11,7 +11,6 @@
 // cudaMalloc'd buffer.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "cother_b200.h"
@@ -32,24 +31,19 @@ constexpr long long kNoAllocMaxColumns = CBP_NOALLOC_MAX_COLUMNS;
 
 static __device__ __align__(256) float g_dp1_strip[5 * kNoAllocMaxColumns];
 
-// Device address of g_dp1_strip per device. In host code the array's name
-// only stands in for it; the address is looked up once per device with that
-// device current.
-constexpr int kMaxDevices = 64;
-float* g_strip_addr[kMaxDevices] = {};
-std::mutex g_strip_mutex;
-
-float* strip_address(int device)
+// Device address of g_dp1_strip on the current device. In host code the
+// array's name only stands in for it. The address is looked up on every
+// call, with the caller's device current, rather than cached: a device reset
+// or a re-created primary context reloads the module at another address.
+// The first lookup on a device loads the module there, which is why the
+// first call should come before any stream capture; later lookups are cheap.
+float* strip_address()
 {
-    std::lock_guard<std::mutex> lock(g_strip_mutex);
-    if (!g_strip_addr[device]) {
-        float* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_dp1_strip);
-        if (e != cudaSuccess)
-            throw cbp::Error(CBP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_strip_addr[device] = ptr;
-    }
-    return g_strip_addr[device];
+    float* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_dp1_strip);
+    if (e != cudaSuccess)
+        throw cbp::Error(CBP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return ptr;
 }
 
 }  // namespace
@@ -74,9 +68,6 @@ extern "C" int cbp_dp1_noalloc(const float* scores, size_t ld, int query_len, co
                                                 std::to_string(kNoAllocMaxColumns) + " columns");
         if (query_len >= 65536)
             throw cbp::Error(CBP_ERR_LIMIT, "cbp_dp1_noalloc: query length must be < 65536");
-        int device = 0;
-        CBP_CUDA(cudaGetDevice(&device));
-        if (device < 0 || device >= kMaxDevices) throw cbp::Error(CBP_ERR_ARG, "cbp_dp1_noalloc: device index");
         cbp::Dp1Args a;
         a.scores = scores;
         a.ld = (long long)ld;
@@ -91,7 +82,7 @@ extern "C" int cbp_dp1_noalloc(const float* scores, size_t ld, int query_len, co
         a.p0 = first_profile;
         a.nprof = nprof;
         a.btck = btck;
-        a.bandbuf = strip_address(device);
+        a.bandbuf = strip_address();
         a.maxsc = max_scores;
         a.maxcoords = max_coords;
         cbp::launch_dp1(a, static_cast<cudaStream_t>(stream));

@@ -132,6 +132,32 @@ class ProfileSet:
             cvnorm2=None if self.cvnorm2 is None else self.cvnorm2[s0:s0 + n].copy(),
         )
 
+    def select(self, indices) -> "ProfileSet":
+        """Profiles `indices` (in that order) as a new set (copies)."""
+        idx = np.asarray(indices, dtype=np.int64)
+        st = self.starts
+        lens = self.lens[idx]
+        pos = np.concatenate([np.arange(st[p], st[p] + self.lens[p]) for p in idx]) \
+            if len(idx) else np.zeros(0, np.int64)
+        tpos = np.concatenate([np.arange(st[p] + p, st[p] + p + self.lens[p] + 1) for p in idx]) \
+            if len(idx) else np.zeros(0, np.int64)
+        return ProfileSet(
+            lens=lens.copy(),
+            bkg=np.ascontiguousarray(self.bkg[:, idx]),
+            eno=self.eno[idx].copy(),
+            trn=np.ascontiguousarray(self.trn[:, tpos]),
+            tf=np.ascontiguousarray(self.tf[:, pos]),
+            dd=np.ascontiguousarray(self.dd[:, pos]),
+            ss=np.ascontiguousarray(self.ss[:, pos]),
+            addrpro=np.repeat(np.arange(len(idx), dtype=np.int32), lens),
+            aa=self.aa[pos].copy(),
+            ssstate=self.ssstate[pos].copy(),
+            names=[self.names[p] for p in idx] if self.names else [],
+            cv=None if self.cv is None else np.ascontiguousarray(self.cv[:, pos]),
+            cvprior=None if self.cvprior is None else self.cvprior[pos].copy(),
+            cvnorm2=None if self.cvnorm2 is None else self.cvnorm2[pos].copy(),
+        )
+
     def field_tables(self):
         """(beg, end) arrays of 181 host pointers, as the reference passes them.
 

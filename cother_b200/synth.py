@@ -230,3 +230,17 @@ def make_workload(name: str, seed: int = 7, ndb: int | None = None, qindex: int 
         add_context_vectors(q, seed * 1000 + 2 + qindex)
     plant_homologs(q, db, homologs, seed=dseed * 1000 + 3 + qindex)
     return q, db
+
+
+def planted_indices(name: str, seed: int = 7, ndb: int | None = None, qindex: int = 0,
+                    homologs: float = HOMOLOG_FRACTION, db_seed: int | None = None) -> np.ndarray:
+    """Indices of the database profiles that make_workload() with the same
+    arguments overwrites with planted homologs (without generating them)."""
+    dseed = seed if db_seed is None else db_seed
+    P = len(db_lengths(name, dseed, ndb))
+    k = int(round(homologs * P))
+    if k <= 0:
+        return np.zeros(0, np.int64)
+    rng = np.random.default_rng(dseed * 1000 + 3 + qindex)
+    return np.sort(rng.choice(P, size=k, replace=False))
+

@@ -253,6 +253,15 @@ int cbp_read_statistics(cbp_context* ctx, float* recs, size_t nmax, size_t* npas
  * (0 stop, 1 left, 2 up, 3 diagonal; src/libmycu/cudp/CuBatchDP_com.h:101-106). */
 int cbp_read_btck(cbp_context* ctx, uint8_t* btck, size_t ld);
 
+/* Columns [first_col, first_col + ncols) of the last slab's matrices, for
+ * inspecting a sample of a slab too large to copy whole: scores, modscores
+ * (float) and phase-1 backtrack codes (uint8), each [query length][ld] on
+ * the host with column 0 = slab column first_col. Any output may be NULL.
+ * An inspection call with no counterpart in the reference (its matrices are
+ * device-internal); CBP_ERR_ARG when the range leaves the slab. */
+int cbp_read_slab_columns(cbp_context* ctx, size_t first_col, size_t ncols, float* scores,
+                          float* modscores, uint8_t* btck, size_t ld);
+
 /* Phase-1 score threshold and log E-value threshold from the E-value
  * threshold and the gapped Karlin-Altschul parameters (the [GAPPED_A_1]
  * lambda and K of cother.par); search space = query_len * db_len.
@@ -420,14 +429,24 @@ int cbp_set_karlin_altschul(cbp_context* ctx, float ungapped_lambda, float ungap
  *              vector of profile p at entry prof_start[p]+p;
  *   prof_len, prof_start  [db_nprof] lengths and first positions;
  *   profiles first_profile .. first_profile+nprof-1 are processed.
+ * Preconditions on every processed profile p (device data, so they are
+ * checked by the kernel, not before the launch): its columns lie inside the
+ * slab, 0 <= prof_start[p] - first_column and
+ * prof_start[p] - first_column + prof_len[p] <= ld, and prof_len[p] < 65536
+ * (cell coordinates are packed into 16 + 16 bits; query_len < 65536 is
+ * checked before the launch, CBP_ERR_LIMIT). A profile that breaks either is
+ * skipped: nothing of it is read or written, its max_scores entry is NaN and
+ * its max_coords entry 0xffffffff.
  * Outputs (device): btck [query_len][ld] backtrack codes, max_scores and
  * max_coords [nprof] (maximum MM score and its cell (x<<16)|y).
  * The work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
  * stream) and the call returns after the launch.
  *
- * The first call on a device looks up the scratch array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. All calls share the one scratch array and it
+ * Every call looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with the caller's device current, so a device reset
+ * between calls is safe. The first lookup on a device loads the library's
+ * device code there: make that first call before any stream capture. All
+ * calls share the one scratch array and it
  * keeps the last call's contents (the DP needs no zeroed scratch: the first
  * band never reads the strip); calls whose work overlaps on the GPU race on
  * it and must be serialised by the caller, e.g. on one stream. */
