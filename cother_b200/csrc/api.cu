@@ -222,11 +222,12 @@ struct cbp_context {
     float cvs_key_first = 0.f, cvs_key_last = 0.f;
     // working buffers
     DevBuf scores, modscores, btck, bandbuf, colorder, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
-    DevBuf hitrecs, statrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf;
+    DevBuf hitrecs, statrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf, dp1err;
     std::vector<char> h_alns[5];
     long long base_len = 0, base_npass = 0;   // running phase-2 offsets over slabs
     long long last_npos2 = 0;
     int h_maperr = 0;   // set by the MAP stage when a wait between warps gave up
+    int h_dp1err = 0;   // set by the phase-1 DP when a staging wait gave up
     bool score_thld_set = false, logE_thld_set = false;
     // results of the last process() call, all slabs
     std::vector<float> h_recs;
@@ -624,6 +625,7 @@ int cbp_create(int device, const cbp_options* opt, const float* ss_table, size_t
             c->opt = *opt;
             CBP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
             for (auto& e : c->ev) CBP_CUDA(cudaEventCreate(&e));
+            dp1_set_attributes();
             std::memcpy(c->sstab_h, ss_table, sizeof(c->sstab_h));
             build_dms_table(c->dmstab_h);
             c->nnweights.reserve(sizeof(kNNWeightsTable));
@@ -655,7 +657,7 @@ int cbp_destroy(cbp_context* c)
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->colorder, &c->dpmax, &c->dpcoords,
                       &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
                       &c->cs2, &c->fb2, &c->sg2, &c->bt2, &c->strip2, &c->maperr, &c->alnbuf,
-                      &c->cvsmap, &c->statrecs})
+                      &c->cvsmap, &c->statrecs, &c->dp1err})
         b->release();
     c->sstab.release();
     c->dmstab.release();
@@ -871,6 +873,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         c->passidx.reserve(maxprof * sizeof(int));
         c->passdst.reserve(maxprof * sizeof(long long));
         c->passcnt.reserve(64);
+        c->dp1err.reserve(sizeof(int));
 
         for (const Slab& s : slabs) {
             ScoreArgs a;
@@ -943,6 +946,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             d.maxcoords = c->dpcoords.as<uint32_t>();
             d.recs = c->dprecs.as<Dp1Rec>();
             d.warps = tn.dp_warps;
+            d.err = c->dp1err.as<int>();
 
             // phase 1 of the slab: column order, score matrix, DP, its
             // finalization and the pass list; with the plain form one CUDA
@@ -958,6 +962,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                                     c->stream);
                 launch_score_matrix(a, c->stream);
                 mark(c->ev[1]);
+                CBP_CUDA(cudaMemsetAsync(c->dp1err.p, 0, sizeof(int), c->stream));
                 launch_dp1(d, c->stream);
                 mark(c->ev[2]);
                 launch_dp1_finalize(d, c->score_thld, c->stream);
@@ -1004,7 +1009,10 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             c->stage_launches[2] += 2;
             int npass = 0;
             CBP_CUDA(cudaMemcpyAsync(&npass, c->passcnt.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CBP_CUDA(cudaMemcpyAsync(&c->h_dp1err, c->dp1err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CBP_CUDA(cudaStreamSynchronize(c->stream));
+            if (c->h_dp1err)
+                throw Error(CBP_ERR_CUDA, "phase-1 DP: a wait for staged score rows timed out");
             float ms = 0.f;
             CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
             c->stage_ms[0] += ms;

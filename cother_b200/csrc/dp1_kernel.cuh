@@ -27,14 +27,18 @@ struct Dp1Args {
     int p0 = 0;                      // first chunk profile of the slab
     int nprof = 0;                   // profiles in the slab
     uint8_t* btck = nullptr;         // [Lq][ld]
-    float* bandbuf = nullptr;        // [5][ld]
+    float* bandbuf = nullptr;        // [5][ld]: the bottom row of a band, for the next
     float* maxsc = nullptr;          // [nprof]
     uint32_t* maxcoords = nullptr;   // [nprof]
     Dp1Rec* recs = nullptr;          // [nprof]
     int warps = 2;                   // warps (profiles) per block of dp1_kernel: 1 or 2
+    int* err = nullptr;              // set to 1 when a staging wait gave up (may be null)
 };
 
 void launch_dp1(const Dp1Args& a, cudaStream_t stream);
+// Per device, before the first launch_dp1 with two warps per block (and
+// outside any stream capture): the shared-memory opt-in of the DP kernels.
+void dp1_set_attributes();
 void launch_dp1_finalize(const Dp1Args& a, float thld, cudaStream_t stream);
 void launch_pass_compact(const Dp1Args& a, int* pass_idx, long long* pass_dst, int* npass,
                          long long* npos, cudaStream_t stream);

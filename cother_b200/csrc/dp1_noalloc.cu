@@ -85,6 +85,7 @@ extern "C" int cbp_dp1_noalloc(const float* scores, size_t ld, int query_len, co
         a.bandbuf = strip_address();
         a.maxsc = max_scores;
         a.maxcoords = max_coords;
+        cbp::dp1_set_attributes();
         cbp::launch_dp1(a, static_cast<cudaStream_t>(stream));
         cbp::set_last_error("");
         return CBP_OK;
