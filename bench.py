@@ -47,7 +47,7 @@ def score_traffic_per_cell(rows: int) -> float:
     return 8.0 + (SCORE_DRAM_BYTES_PER_CELL - 8.0) * 32.0 / rows
 
 
-STAGES = ["score_matrix", "phase1_dp", "phase1_finalize", "statistics", "map_realignment"]
+STAGES = ["score_matrix", "phase1_dp", "phase1_finalize", "statistics", "map_realignment", "hit_order"]
 OPS_PER_DDMS_STEP = 50  # algorithmic ops of one 4-cell DDMS step (2 pair scores,
                         # 2 interpolations, 4 segment updates, 1 top-3 register)
 

@@ -86,6 +86,7 @@ def load_library(path: str | None = None):
                                   ctypes.POINTER(sz)]),
         "cbp_read_btck": (i32, [vp, vp, sz]),
         "cbp_read_slab_columns": (i32, [vp, sz, sz, vp, vp, vp, sz]),
+        "cbp_read_fits": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_score_threshold": (None, [sz, ctypes.c_uint64, f32, f32, f32, ctypes.POINTER(f32),
                                        ctypes.POINTER(f32)]),
         "cbp_get_hit_records": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
@@ -301,6 +302,18 @@ class BatchProcessing:
             _check(L.cbp_read_statistics(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
         return out
 
+    def read_fits(self) -> np.ndarray:
+        """The precision forms: per passed pair of the last slab, the
+        parameter fit in FP64 and in FP32, float64 [npass][8] (lambda, K, H,
+        expected score of each; cbp_read_fits)."""
+        L = load_library()
+        n = ctypes.c_size_t()
+        _check(L.cbp_read_fits(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 8), np.float64)
+        if n.value:
+            _check(L.cbp_read_fits(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out
+
     def read_phase1(self):
         """Phase-1 records of the last slab: dict of arrays (score, psts,
         beg, end, passed) and the pass list."""
@@ -359,16 +372,18 @@ class BatchProcessing:
             out.append(tuple(bytes(rows[r, term - n:term]).decode() for r in range(5)))
         return out
 
-    def hit_list(self) -> np.ndarray:
+    def hit_list(self, top: int | None = None) -> np.ndarray:
         """Record indices of the reported hits of the last search (log E at
-        most the threshold, realigned), sorted by log E-value: the order of
-        the reference's finalizer."""
+        most the threshold, realigned), sorted by log E-value on the device:
+        the order of the reference's finalizer. With `top`, only the first
+        `top` (the top-k hits)."""
         L = load_library()
         n = ctypes.c_size_t()
         _check(L.cbp_get_hit_list(self._h, None, 0, ctypes.byref(n)))
-        out = np.zeros(n.value, np.int32)
-        if n.value:
-            _check(L.cbp_get_hit_list(self._h, out.ctypes.data, n.value, ctypes.byref(n)))
+        k = n.value if top is None else min(int(top), n.value)
+        out = np.zeros(k, np.int32)
+        if k:
+            _check(L.cbp_get_hit_list(self._h, out.ctypes.data, k, ctypes.byref(n)))
         return out
 
     def search_space(self):

@@ -34,6 +34,7 @@ CUDA_SOURCES = [
     "map_kernel.cu",
     "dp1_noalloc.cu",
     "tc_kernel.cu",
+    "hits_kernel.cu",
     "format.cpp",
     "dbfile.cpp",
 ]
@@ -46,6 +47,7 @@ CUDA_HEADERS = [
     "score_kernel.cuh",
     "dp1_kernel.cuh",
     "tc_kernel.cuh",
+    "hits_kernel.cuh",
 ]
 
 

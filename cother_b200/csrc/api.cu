@@ -20,13 +20,15 @@
 #include "score_kernel.cuh"
 #include "tc_kernel.cuh"
 #include "dp1_kernel.cuh"
+#include "hits_kernel.cuh"
 #include "stats_kernel.cuh"
 #include "map_kernel.cuh"
 
 namespace cbp {
 
 // format.cpp: the finalizer's per-hit text from host records and rows
-int format_hits_from(const float* recs, size_t nrecs, const char* rows, size_t row_stride, size_t row_length,
+int format_hits_from(const float* recs, size_t nrecs, const int32_t* order, size_t norder, const char* rows,
+                     size_t row_stride, size_t row_length,
                      const int* prof_len, const float* prof_eno, const uint8_t* prof_ss, size_t nprof,
                      const char* const* descs, int query_len, float query_eno, int query_ss, float ssswgt,
                      float logevthld, float sspace, const cbp_format_options* fo, char* buf, size_t cap,
@@ -223,6 +225,9 @@ struct cbp_context {
     // working buffers
     DevBuf scores, modscores, btck, bandbuf, colorder, dpmax, dpcoords, dprecs, passidx, passdst, passcnt;
     DevBuf hitrecs, statrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf, dp1err;
+    DevBuf hitkeys, hitcnt;    // sort keys of all records of a query, reported count
+    DevBuf fits;               // the precision forms: FP64 and FP32 parameter fits per passed pair
+    std::vector<int32_t> h_order;   // reported hits in the finalizer's order (sorted on the device)
     std::vector<char> h_alns[5];
     long long base_len = 0, base_npass = 0;   // running phase-2 offsets over slabs
     long long last_npos2 = 0;
@@ -657,7 +662,7 @@ int cbp_destroy(cbp_context* c)
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->colorder, &c->dpmax, &c->dpcoords,
                       &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
                       &c->cs2, &c->fb2, &c->sg2, &c->bt2, &c->strip2, &c->maperr, &c->alnbuf,
-                      &c->cvsmap, &c->statrecs, &c->dp1err})
+                      &c->cvsmap, &c->statrecs, &c->dp1err, &c->hitkeys, &c->hitcnt, &c->fits})
         b->release();
     c->sstab.release();
     c->dmstab.release();
@@ -834,6 +839,7 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         for (float& m : c->stage_ms) m = 0.f;
         for (uint64_t& m : c->stage_launches) m = 0;
         c->h_recs.clear();
+        c->h_order.clear();
         for (auto& r : c->h_alns) r.clear();
         c->base_len = 0;
         c->base_npass = 0;
@@ -874,6 +880,9 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
         c->passdst.reserve(maxprof * sizeof(long long));
         c->passcnt.reserve(64);
         c->dp1err.reserve(sizeof(int));
+        c->hitkeys.reserve((size_t)hit_sort_capacity(c->db->view.P) * sizeof(uint64_t));
+        c->hitcnt.reserve(sizeof(int));
+        CBP_CUDA(cudaMemsetAsync(c->hitcnt.p, 0, sizeof(int), c->stream));
 
         for (const Slab& s : slabs) {
             ScoreArgs a;
@@ -1052,6 +1061,12 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 st.ref_K = c->ref_K;
                 st.exp_gapped_lambda = c->gap_lambda;
                 st.exp_gapped_K = c->gap_K;
+                if (c->opt.tc_form != CBP_TC_PLAIN) {
+                    // the precision forms fit lambda, K, H in FP64 for the E-values
+                    c->fits.reserve((size_t)npass * kFitDoubles * sizeof(double));
+                    st.fits = c->fits.as<double>();
+                    st.use_fit64 = 1;
+                }
                 CBP_CUDA(cudaEventRecord(c->ev[4], c->stream));
                 launch_stats(st, npass, c->stream);
                 CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
@@ -1128,6 +1143,10 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                     c->stage_launches[4] += 1;
                 }
                 c->last_npos2 = npos2;
+                // sort keys of this slab's records, for the hit order
+                c->launches += launch_hit_keys(c->hitrecs.as<float>(), npass, c->logE_thld, c->base_npass,
+                                               c->hitkeys.as<uint64_t>(), c->hitcnt.as<int>(), c->stream);
+                c->stage_launches[5] += 1;
                 const size_t off = c->h_recs.size();
                 c->h_recs.resize(off + (size_t)npass * kRecFloats);
                 CBP_CUDA(cudaMemcpyAsync(c->h_recs.data() + off, c->hitrecs.p,
@@ -1162,6 +1181,29 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 c->base_len += npos2;
                 c->base_npass += npass;
             }
+        }
+        // the reported hits in the finalizer's order: one sort over the keys
+        // of all records; the reported ones come first
+        if (c->base_npass > 0) {
+            CBP_CUDA(cudaEventRecord(c->ev[4], c->stream));
+            const int nl = launch_hit_sort(c->hitkeys.as<uint64_t>(), c->base_npass, c->stream);
+            CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
+            c->launches += nl;
+            c->stage_launches[5] += nl;
+            int nrep = 0;
+            CBP_CUDA(cudaMemcpyAsync(&nrep, c->hitcnt.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CBP_CUDA(cudaStreamSynchronize(c->stream));
+            if (nrep < 0 || nrep > c->base_npass) throw Error(CBP_ERR_CUDA, "hit order: inconsistent count");
+            std::vector<uint64_t> keys((size_t)nrep);
+            if (nrep > 0)
+                CBP_CUDA(cudaMemcpyAsync(keys.data(), c->hitkeys.p, (size_t)nrep * sizeof(uint64_t),
+                                         cudaMemcpyDeviceToHost, c->stream));
+            CBP_CUDA(cudaStreamSynchronize(c->stream));
+            c->h_order.resize((size_t)nrep);
+            for (int i = 0; i < nrep; i++) c->h_order[i] = (int32_t)(uint32_t)keys[i];
+            float ms = 0.f;
+            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+            c->stage_ms[5] += ms;
         }
         CBP_CUDA(cudaStreamSynchronize(c->stream));
     });
@@ -1231,6 +1273,21 @@ int cbp_read_statistics(cbp_context* c, float* recs, size_t nmax, size_t* npass)
     });
 }
 
+int cbp_read_fits(cbp_context* c, double* fits, size_t nmax, size_t* npass)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!c->last_Lq) throw Error(CBP_ERR_STATE, "no processed query");
+        if (c->opt.tc_form == CBP_TC_PLAIN) throw Error(CBP_ERR_STATE, "the plain form fits in FP32 only");
+        const size_t n = (size_t)c->last_npass;
+        if (npass) *npass = n;
+        if (!fits || n == 0) return;
+        if (nmax < n) throw Error(CBP_ERR_ARG, "output array too small");
+        CBP_CUDA(cudaStreamSynchronize(c->stream));
+        CBP_CUDA(cudaMemcpy(fits, c->fits.p, n * kFitDoubles * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
 int cbp_read_btck(cbp_context* c, uint8_t* btck, size_t ld)
 {
     return guarded([&] {
@@ -1283,23 +1340,11 @@ int cbp_get_hit_list(cbp_context* c, int32_t* order, size_t max_hits, size_t* nh
 {
     return guarded([&] {
         check_ctx(c);
-        const size_t n = c->h_recs.size() / kRecFloats;
-        std::vector<int32_t> idx;
-        for (size_t i = 0; i < n; i++) {
-            const float* r = c->h_recs.data() + i * kRecFloats;
-            int32_t alnlen;
-            std::memcpy(&alnlen, &r[rEpA], 4);
-            if (r[rEvalue] <= c->logE_thld && alnlen >= 1) idx.push_back((int32_t)i);
-        }
-        std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) {
-            return c->h_recs[(size_t)a * kRecFloats + rEvalue] <
-                   c->h_recs[(size_t)b * kRecFloats + rEvalue];
-        });
-        if (nhits) *nhits = idx.size();
-        if (order) {
-            if (max_hits < idx.size()) throw Error(CBP_ERR_ARG, "hit buffer too small");
-            std::memcpy(order, idx.data(), idx.size() * sizeof(int32_t));
-        }
+        // ordered on the device at the end of cbp_process; the first
+        // max_hits entries are the top max_hits hits
+        const size_t n = c->h_order.size();
+        if (nhits) *nhits = n;
+        if (order && n) std::memcpy(order, c->h_order.data(), std::min(n, max_hits) * sizeof(int32_t));
     });
 }
 
@@ -1329,7 +1374,8 @@ int cbp_format_hits(cbp_context* c, const cbp_format_options* fo, const char* co
         for (int r = 0; r < 5; r++)
             if (n) std::memcpy(rows.data() + (size_t)r * n, c->h_alns[r].data(), n);
         const int qss = c->query.h_ss.empty() ? 1 : c->query.h_ss[0];
-        rc = format_hits_from(c->h_recs.data(), c->h_recs.size() / kRecFloats, rows.data(), n, n,
+        rc = format_hits_from(c->h_recs.data(), c->h_recs.size() / kRecFloats, c->h_order.data(),
+                              c->h_order.size(), rows.data(), n, n,
                               db.h_plen.data(), db.h_eno.data(), db.h_ss.empty() ? nullptr : db.h_ss.data(),
                               db.h_plen.size(), descs, c->last_Lq, c->query_eno, qss, c->opt.ssswgt,
                               c->logE_thld, (float)c->searchspace, fo, buf, cap, used, nhits);

@@ -488,10 +488,21 @@ void check_format_options(const cbp_format_options* fo)
 }
 
 // the packed records: annotation NUL hit-record NUL, per reported hit
-std::string format_hits(const HitsInput& in, const cbp_format_options& fo, size_t* nhits)
+std::string format_hits(const HitsInput& in, const cbp_format_options& fo, size_t* nhits,
+                        const int32_t* order = nullptr, size_t norder = 0)
 {
     std::string out;
-    const std::vector<size_t> idx = reported(in);
+    // the order given (the device's) or the finalizer's, restated
+    std::vector<size_t> idx;
+    if (order) {
+        for (size_t i = 0; i < norder; i++) {
+            if (order[i] < 0 || (size_t)order[i] >= in.nrecs)
+                throw FormatError{CBP_ERR_ARG, "hit order names a record outside the records"};
+            idx.push_back((size_t)order[i]);
+        }
+    } else {
+        idx = reported(in);
+    }
     for (size_t k : idx) {
         const HitView h = view_of(in, k);
         std::string annot, rec;
@@ -788,7 +799,8 @@ int guarded_fmt(F&& f)
 
 // used by api.cu for the context's own results
 namespace cbp {
-int format_hits_from(const float* recs, size_t nrecs, const char* rows, size_t row_stride, size_t row_length,
+int format_hits_from(const float* recs, size_t nrecs, const int32_t* order, size_t norder, const char* rows,
+                     size_t row_stride, size_t row_length,
                      const int* prof_len, const float* prof_eno, const uint8_t* prof_ss, size_t nprof,
                      const char* const* descs, int query_len, float query_eno, int query_ss, float ssswgt,
                      float logevthld, float sspace, const cbp_format_options* fo, char* buf, size_t cap,
@@ -799,7 +811,7 @@ int format_hits_from(const float* recs, size_t nrecs, const char* rows, size_t r
         HitsInput in{recs, nrecs, rows, row_stride, row_length, prof_len, prof_eno, prof_ss, nprof,
                      descs, query_len, query_eno, query_ss, ssswgt, logevthld, sspace};
         size_t n = 0;
-        const std::string s = format_hits(in, *fo, &n);
+        const std::string s = format_hits(in, *fo, &n, order, norder);
         if (nhits) *nhits = n;
         return deliver(s, buf, cap, used);
     });
@@ -825,7 +837,7 @@ int cbp_format_hits_host(const cbp_hits_input* in, const cbp_format_options* fo,
         cbp::set_last_error("cbp_format_hits_host: null input");
         return CBP_ERR_ARG;
     }
-    return cbp::format_hits_from(in->recs, in->nrecs, in->rows, in->row_stride, in->row_length, in->prof_len,
+    return cbp::format_hits_from(in->recs, in->nrecs, nullptr, 0, in->rows, in->row_stride, in->row_length, in->prof_len,
                                  in->prof_eno, in->prof_ss, in->nprof, in->descs, in->query_len, in->query_eno,
                                  in->query_ss, in->ssswgt, in->log_evalue_threshold, in->search_space, fo, buf,
                                  cap, used, nhits);

@@ -328,6 +328,199 @@ __device__ void significance(const StatsArgs& a, int Lq, int Ld, float qeno, flo
     out4[3] = epa;
 }
 
+// ---- the parameter fit in FP64 (the precision forms)
+//
+// The same estimation as the FP32 steps below -- expected score, lambda by
+// Newton steps guarded by bisection, relative entropy, K by convolution on
+// the 21 x 32 grid, with the reference's constants, guards and stopping
+// rules -- restated in double precision from the pair's integer histogram.
+// exp is the CUDA double-precision exp. Block-wide sums are per row by the
+// shuffle-down tree and then over the rows, as in FP32.
+struct Fit64 {
+    double lambda, K, H, E;   // lambda unscaled, E unscaled
+};
+
+__device__ __forceinline__ double wsum_down64(double v)
+{
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    return v;
+}
+
+// valid in thread 0; all threads call (barriers)
+__device__ __forceinline__ double grid_sum64(double v, double* tmp)
+{
+    const int y = threadIdx.x >> 5, x = threadIdx.x & 31;
+    v = wsum_down64(v);
+    if (x == 0) tmp[y] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (y == 0) {
+        t = (x < NS) ? tmp[x] : 0.0;
+        t = wsum_down64(t);
+    }
+    __syncthreads();
+    return t;
+}
+
+__device__ Fit64 fit64(const int* cnt, int left, int right, float minscf, float maxscf, int minu, int maxu,
+                       double (*g)[33], double* up, double* tmp, double* sh, int* flag)
+{
+    const int tid = threadIdx.x;
+    const int y = tid >> 5, x = tid & 31;
+    const double LSMIN = (double)kLogSpMin, LSMAX = (double)kLogSpMax;
+    double gv = (x + left <= right) ? (double)cnt[left + x] : 0.0;
+    const double scx = (double)(left + x - 320);
+    const double minsc = (double)minscf, maxsc = (double)maxscf;
+    // probabilities
+    {
+        const double rs = wsum_down64(gv);
+        if (x == 0) tmp[y] = rs;
+        __syncthreads();
+        if (y == 0) {
+            double t = (x < NS) ? tmp[x] : 0.0;
+            t = wsum_down64(t);
+            if (x == 0) sh[0] = t;
+        }
+        __syncthreads();
+        if (y == 0 && x < NS) up[x] = tmp[x] / sh[0];
+        gv = gv / sh[0];
+        __syncthreads();
+    }
+    g[y][x] = gv;
+    double E = grid_sum64(scx * gv, tmp);
+    if (tid == 0) sh[1] = E;
+    __syncthreads();
+    E = sh[1];
+    // lambda (CuBatchSS_lambda.cuh:80-330)
+    double lambda = -1.0;
+    if (!(0.0 <= E || maxsc <= 0.0)) {
+        auto eq = [&](double lx, double& f, double& df) {
+            double lf = 0.0, ldf = 0.0;
+            if (minsc <= scx && scx <= maxsc) {
+                const double s = scx - maxsc;
+                const double yy = lx * s;
+                if (LSMIN < yy) { lf = exp(yy) * gv; ldf = lf * s; }
+            }
+            double F = grid_sum64(lf, tmp);
+            double D = grid_sum64(ldf, tmp + 32);
+            double xm = lx * -maxsc;
+            if (LSMIN < xm) { xm = exp(xm); F = F - xm; D = D + xm * maxsc; }
+            f = F;
+            df = D;
+        };
+        const double X1 = 1.0e-5, X2 = 10.0;
+        double f, df, fl, dd, dx, dxold, xh, xl, rts;
+        eq(X1, fl, dd);
+        eq(X2, f, dd);
+        if (tid == 0) *flag = (fl > 0.0 && f > 0.0) || (fl < 0.0 && f < 0.0);
+        __syncthreads();
+        if (!*flag) {
+            if (fl < 0.0) { xl = X1; xh = X2; } else { xh = X1; xl = X2; }
+            rts = 0.5 * (X1 + X2);
+            dxold = fabs(X2 - X1);
+            dx = dxold;
+            eq(rts, f, df);
+            int n;
+            for (n = 0; n < 32; n++) {
+                __syncthreads();
+                if (tid == 0) {
+                    int stop = 0;
+                    if ((((rts - xh) * df - f) * ((rts - xl) * df - f) > 0.0) || (fabs(2.0 * f) > fabs(dxold * df))) {
+                        dxold = dx;
+                        dx = 0.5 * (xh - xl);
+                        rts = xl + dx;
+                        if (xl == rts) stop = 1;
+                    } else {
+                        dxold = dx;
+                        dx = f / df;
+                        const double temp = rts;
+                        rts = rts - dx;
+                        if (temp == rts) stop = 1;
+                    }
+                    if (fabs(dx) < 1.0e-4) stop = 1;
+                    *flag = stop;
+                    sh[2] = rts;
+                }
+                __syncthreads();
+                rts = sh[2];
+                const int stop = *flag;
+                __syncthreads();
+                if (stop) break;
+                eq(rts, f, df);
+                if (f < 0.0) xl = rts; else xh = rts;
+            }
+            lambda = (n == 32) ? -1.0 : rts;
+        }
+        if (tid == 0) sh[3] = lambda;
+        __syncthreads();
+        lambda = sh[3];
+    }
+    // relative entropy (CuBatchSS_entropy.cuh:14-70)
+    double H = -1.0;
+    if (lambda > 0.0) {
+        double e = 0.0;
+        if (minsc <= scx && scx <= maxsc) {
+            const double yy = lambda * scx;
+            if (LSMIN < yy && yy < LSMAX - 3.0) e = exp(yy) * yy * gv;
+        }
+        H = grid_sum64(e, tmp);
+        if (tid == 0) sh[4] = H;
+        __syncthreads();
+        H = sh[4];
+    }
+    if (y == 0) g[10][x] = 1.0;
+    lambda = lambda * 32.0;
+    E = E / 32.0;
+    __syncthreads();
+    // K (CuBatchSS_K.cuh:49-320)
+    double K = -1.0;
+    if (!(0.0 <= E || lambda <= 0.0 || H <= 0.0)) {
+        if (minu == -1 && maxu == 1) {
+            const double minprb = up[-1 + 10], maxprb = up[1 + 10];
+            const double d = minprb - maxprb;
+            K = d * d / minprb;
+        } else if (minu == -1 || maxu == 1) {
+            if (maxu != 1) K = (lambda / H) * (1.0 - exp(-lambda)) * (E * E);
+            else K = (H / lambda) * (1.0 - exp(-lambda));
+        } else {
+            const int range = maxu - minu + 1;
+            const int isc = left + x - 320;
+            double sigma = 0.0, Pj = 1.0;
+            int mins = minu, maxs = maxu;
+            for (int j = 1; j <= 32 && 1.0e-4 < Pj; j++) {
+                double pji = 0.0, pv = 0.0;
+                if (mins <= isc && isc <= maxs && -32 <= isc && isc <= 32) {
+                    const double etols = isc < 0 ? lambda * (double)isc : 0.0;
+                    if (LSMIN < etols) {
+                        const int lo = (maxs - isc < range) ? maxu - (maxs - isc) : minu;
+                        const int hi = (isc - mins < range) ? minu + (isc - mins) : maxu;
+                        for (int i = lo; i <= hi; i++) {
+                            int yy = y, xx = x - i;
+                            if (32 <= xx) { xx -= 32; if (yy + 1 < NS) yy++; else continue; }
+                            else if (xx < 0) { xx += 32; if (0 < yy) yy--; else continue; }
+                            pji = fma(g[yy][xx], up[i + 10], pji);
+                        }
+                        pv = pji * exp(etols);
+                    }
+                }
+                __syncthreads();       // every read of the previous grid is done
+                g[y][x] = pji;
+                const double P = grid_sum64(pv, tmp);
+                if (tid == 0) {
+                    sigma = sigma + P / (double)j;
+                    sh[5] = P;
+                }
+                __syncthreads();
+                Pj = sh[5];
+                mins += minu;
+                maxs += maxu;
+            }
+            if (tid == 0) K = lambda * exp(-2.0 * sigma) / (H * (1.0 - exp(-lambda)));
+        }
+    }
+    return Fit64{lambda, K, H, E};
+}
+
 __global__ void __launch_bounds__(kThreads)
 stats_kernel(const StatsArgs a)
 {
@@ -549,6 +742,27 @@ stats_kernel(const StatsArgs a)
             }
             if (tid == 0)
                 K = __fdiv_rn(lambda * cb_expf(-2.0f * sigma), H * (1.0f - cb_expf(-lambda)));
+        }
+    }
+
+    // 7b. the precision forms: the fit again in FP64, used for the E-value
+    if (a.fits) {
+        __shared__ double g64[NS][33];
+        __shared__ double up64[NS];
+        __shared__ double tmp64[64];
+        __shared__ double sh64[8];
+        __syncthreads();
+        const Fit64 f = fit64(cnt, left, right, minsc, maxsc, minu, maxu, g64, up64, tmp64, sh64, &flag);
+        if (tid == 0) {
+            double* o = a.fits + (long long)k * kFitDoubles;
+            o[0] = f.lambda; o[1] = f.K; o[2] = f.H; o[3] = f.E;
+            o[4] = lambda; o[5] = K; o[6] = H; o[7] = E;
+            if (a.use_fit64) {
+                lambda = (float)f.lambda;
+                K = (float)f.K;
+                H = (float)f.H;
+                E = (float)f.E;
+            }
         }
     }
 

@@ -36,7 +36,14 @@ struct StatsArgs {
     float searchspace = 0.f;
     float ref_lambda = 0.f, ref_K = 0.f;
     float exp_gapped_lambda = 0.f, exp_gapped_K = 0.f;
+    // the precision forms: per pair, the parameter fit in FP64 and in FP32
+    // (kFitDoubles each: lambda, K, H, E in FP64, then in FP32); with
+    // use_fit64 the E-value and the record take the FP64 fit's parameters
+    double* fits = nullptr;
+    int use_fit64 = 0;
 };
+
+constexpr int kFitDoubles = 8;
 
 void launch_stats(const StatsArgs& a, int npass, cudaStream_t stream);
 

@@ -249,6 +249,16 @@ int cbp_read_phase1(cbp_context* ctx, float* score, float* psts, uint32_t* beg,
  * src/libmycu/cupro/CuBatchProcessing.cu:430-480). */
 int cbp_read_statistics(cbp_context* ctx, float* recs, size_t nmax, size_t* npass);
 
+/* The precision forms (tc_form != CBP_TC_PLAIN) fit the statistical
+ * parameters of each passed pair twice, in FP64 (used for its E-value) and
+ * in FP32 (the reference's arithmetic); this returns both for the passed
+ * pairs of the last slab, 8 doubles each: lambda, K, H, expected score of
+ * the FP64 fit, then the same of the FP32 fit (lambda and the expected score
+ * per unscaled score unit). No counterpart in the reference, whose fit is
+ * FP32 only (src/libmycu/cuss/CuBatchSS_lambda.cuh:80-330, CuBatchSS_K.cuh,
+ * CuBatchSS_entropy.cuh). CBP_ERR_STATE in the plain form. */
+int cbp_read_fits(cbp_context* ctx, double* fits, size_t nmax, size_t* npass);
+
 /* Backtrack codes of the last slab's phase-1 DP, btck[r * ld + c]
  * (0 stop, 1 left, 2 up, 3 diagonal; src/libmycu/cudp/CuBatchDP_com.h:101-106). */
 int cbp_read_btck(cbp_context* ctx, uint8_t* btck, size_t ld);
@@ -303,8 +313,11 @@ int cbp_get_alignments(cbp_context* ctx, char* rows, size_t row_stride, size_t* 
  * threshold and that were realigned (alignment length >= 1)
  * (src/libmycu/cupro/CuBatchProcessingFinalizerPlain.cpp:79-92), sorted by
  * log E-value, smallest first (CuBatchProcessingFinalizer.cpp:283-292; equal
- * values keep database order). order[i] receives the record index of the
- * i-th hit; with order == NULL only the count is returned. */
+ * values keep database order). The order is computed on the device (a sort
+ * of all records' keys at the end of cbp_process). *nhits receives the
+ * number of reported hits; order[i] receives the record index of the i-th,
+ * for i < min(max_hits, *nhits): the top max_hits hits. With order == NULL
+ * only the count is returned. */
 int cbp_get_hit_list(cbp_context* ctx, int32_t* order, size_t max_hits, size_t* nhits);
 
 /* Effective search space and length adjustment of the last cbp_process()

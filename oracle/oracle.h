@@ -146,6 +146,8 @@ void orc_score_histogram(int Lq, int Ld, const float* S, long long lds, const ch
 
 /* out[6] = min, max, E, H, lambda, K; up[21] = unscaled probabilities */
 void orc_stat_params(const int* counts, float* out, float* up);
+/* the same fit in FP64: out[0..3] = lambda (unscaled), K, H, expected score */
+void orc_stat_params64(const int* counts, double* out);
 
 typedef struct orc_sig_params {
     int ssemodel;

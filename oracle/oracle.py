@@ -278,6 +278,8 @@ def _stats_lib():
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.orc_stat_params.restype = None
         L.orc_stat_params.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_stat_params64.restype = None
+        L.orc_stat_params64.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_significance.restype = None
         L.orc_significance.argtypes = [ctypes.POINTER(SigParams), ctypes.c_int, ctypes.c_int,
                                        ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -306,6 +308,30 @@ def length_adjustment(m, n, N):
     _stats_lib().orc_length_adjustment(par["Lambda"], par["K"], par["Alpha"], par["Beta"], int(m),
                                        int(n), int(N), ctypes.byref(ss), ctypes.byref(dl))
     return ss.value, dl.value
+
+
+def stat_params64(counts):
+    """The parameter fit in FP64 from a pair's score histogram (641 counts):
+    (lambda, K, H, expected score), lambda and the expected score per
+    unscaled score unit."""
+    c = np.ascontiguousarray(counts, np.int32)
+    out = np.zeros(4, np.float64)
+    _stats_lib().orc_stat_params64(c.ctypes.data, out.ctypes.data)
+    return out
+
+
+def significance(Lq, Ld, qeno, deno, score, psts, lam, K, searchspace, ssemodel=2):
+    """(lambda_est, K_est, logE, logEpA) of a pair from given lambda and K
+    (the FP32 E-value computation)."""
+    L = _stats_lib()
+    par = cother_par()
+    w = nn_weights()
+    sp = SigParams(int(ssemodel), float(searchspace), par["UNGAPPED"]["Lambda"], par["UNGAPPED"]["K"],
+                   par["GAPPED_A_1"]["Lambda"], par["GAPPED_A_1"]["K"], w.ctypes.data)
+    o4 = np.zeros(4, np.float32)
+    L.orc_significance(ctypes.byref(sp), int(Lq), int(Ld), float(qeno), float(deno), float(score),
+                       float(psts), float(lam), float(K), o4.ctypes.data)
+    return o4
 
 
 def pair_statistics(S, qaa, daa, score, psts, Lq, Ld, qeno, deno, searchspace, ssemodel=2,

@@ -360,6 +360,181 @@ void orc_stat_params(const int* counts, float* out, float* up)
 }
 
 /* ------------------------------------------------------------------------
+ * The parameter fit in FP64: the same estimation as orc_stat_params (the
+ * reference's equations, constants, guards and stopping rules:
+ * src/libmycu/cuss/CuBatchSS_expected.cuh, CuBatchSS_lambda.cuh:80-330,
+ * CuBatchSS_entropy.cuh:14-70, CuBatchSS_K.cuh:49-320) in double precision
+ * with the C library's exp, sums taken in plain loop order. The checker of
+ * the CUDA path's FP64 fit (the precision forms) and the FP64 side of the
+ * FP32 fit's error report.
+ * out[0..3] = lambda (unscaled), K, H, expected score (unscaled).
+ */
+static void lmbd_eq64(double x, double g[NS][32], const int* left, double minsc, double maxsc,
+                      double* f, double* df)
+{
+    double F = 0.0, DF = 0.0;
+    for (int y = 0; y < NS; y++)
+        for (int t = 0; t < 32; t++) {
+            double sc = (double)(left[y] + t - 320);
+            if (minsc <= sc && sc <= maxsc) {
+                sc = sc - maxsc;
+                double yy = x * sc;
+                if ((double)LOG_SP_MIN < yy) {
+                    double a = exp(yy) * g[y][t];
+                    F += a;
+                    DF += a * sc;
+                }
+            }
+        }
+    double xm = x * -maxsc;
+    if ((double)LOG_SP_MIN < xm) {
+        xm = exp(xm);
+        F = F - xm;
+        DF = DF + xm * maxsc;
+    }
+    *f = F;
+    if (df) *df = DF;
+}
+
+void orc_stat_params64(const int* counts, double* out)
+{
+    double g[NS][32], up[NS];
+    int left[NS], right[NS];
+    double total = 0.0;
+    for (int y = 0; y < NS; y++) {
+        row_interval(y, &left[y], &right[y]);
+        for (int t = 0; t < 32; t++) {
+            g[y][t] = (t + left[y] <= right[y]) ? (double)counts[left[y] + t] : 0.0;
+            total += g[y][t];
+        }
+    }
+    for (int y = 0; y < NS; y++) {
+        double rs = 0.0;
+        for (int t = 0; t < 32; t++) rs += g[y][t];
+        up[y] = rs / total;
+    }
+    double E = 0.0, mins = 0.0, maxs = 0.0;
+    for (int y = 0; y < NS; y++)
+        for (int t = 0; t < 32; t++) {
+            g[y][t] = g[y][t] / total;
+            double sc = (double)(left[y] + t - 320);
+            E += sc * g[y][t];
+            if (g[y][t] != 0.0) {
+                if (sc < mins) mins = sc;
+                if (sc > maxs) maxs = sc;
+            }
+        }
+    /* lambda */
+    double lambda = -1.0;
+    if (!(0.0 <= E || maxs <= 0.0)) {
+        const double X1 = 1.0e-5, X2 = 10.0;
+        double f, df, fl, dx, dxold, xh, xl, rts;
+        lmbd_eq64(X1, g, left, mins, maxs, &fl, 0);
+        lmbd_eq64(X2, g, left, mins, maxs, &f, 0);
+        if (!((fl > 0.0 && f > 0.0) || (fl < 0.0 && f < 0.0))) {
+            if (fl < 0.0) { xl = X1; xh = X2; } else { xh = X1; xl = X2; }
+            rts = 0.5 * (X1 + X2);
+            dxold = fabs(X2 - X1);
+            dx = dxold;
+            lmbd_eq64(rts, g, left, mins, maxs, &f, &df);
+            int n;
+            for (n = 0; n < 32; n++) {
+                int stop = 0;
+                if ((((rts - xh) * df - f) * ((rts - xl) * df - f) > 0.0) || (fabs(2.0 * f) > fabs(dxold * df))) {
+                    dxold = dx;
+                    dx = 0.5 * (xh - xl);
+                    rts = xl + dx;
+                    if (xl == rts) stop = 1;
+                } else {
+                    dxold = dx;
+                    dx = f / df;
+                    double temp = rts;
+                    rts = rts - dx;
+                    if (temp == rts) stop = 1;
+                }
+                if (fabs(dx) < 1.0e-4) stop = 1;
+                if (stop) break;
+                lmbd_eq64(rts, g, left, mins, maxs, &f, &df);
+                if (f < 0.0) xl = rts; else xh = rts;
+            }
+            lambda = (n == 32) ? -1.0 : rts;
+        }
+    }
+    /* relative entropy */
+    double H = -1.0;
+    if (lambda > 0.0) {
+        H = 0.0;
+        for (int y = 0; y < NS; y++)
+            for (int t = 0; t < 32; t++) {
+                double sc = (double)(left[y] + t - 320);
+                if (mins <= sc && sc <= maxs) {
+                    double yy = lambda * sc;
+                    if ((double)LOG_SP_MIN < yy && yy < (double)LOG_SP_MAX - 3.0) H += exp(yy) * yy * g[y][t];
+                }
+            }
+    }
+    for (int t = 0; t < 32; t++) g[10][t] = 1.0;
+    lambda = lambda * 32.0;
+    E = E / 32.0;
+    int minu = 0, maxu = 0;
+    for (int t = 0; t < NS; t++)
+        if (up[t] != 0.0) {
+            if (t - 10 < minu) minu = t - 10;
+            if (t - 10 > maxu) maxu = t - 10;
+        }
+    /* K */
+    double K = -1.0;
+    if (!(0.0 <= E || lambda <= 0.0 || H <= 0.0)) {
+        if (minu == -1 && maxu == 1) {
+            double minprb = up[-1 + 10], maxprb = up[1 + 10];
+            double d = minprb - maxprb;
+            K = d * d / minprb;
+        } else if (minu == -1 || maxu == 1) {
+            if (maxu != 1) K = (lambda / H) * (1.0 - exp(-lambda)) * (E * E);
+            else K = (H / lambda) * (1.0 - exp(-lambda));
+        } else {
+            const int range = maxu - minu + 1;
+            double sigma = 0.0, Pj = 1.0;
+            int mn = minu, mx = maxu;
+            double nxt[NS][32];
+            for (int j = 1; j <= 32 && 1.0e-4 < Pj; j++) {
+                double P = 0.0;
+                for (int y = 0; y < NS; y++)
+                    for (int t = 0; t < 32; t++) {
+                        double pji = 0.0;
+                        int sc = left[y] + t - 320;
+                        if (mn <= sc && sc <= mx && -32 <= sc && sc <= 32) {
+                            double etols = sc < 0 ? lambda * (double)sc : 0.0;
+                            if ((double)LOG_SP_MIN < etols) {
+                                int lo = (mx - sc < range) ? maxu - (mx - sc) : minu;
+                                int hi = (sc - mn < range) ? minu + (sc - mn) : maxu;
+                                for (int i = lo; i <= hi; i++) {
+                                    int yy = y, xx = t - i;
+                                    if (32 <= xx) { xx -= 32; if (yy + 1 < NS) yy++; else continue; }
+                                    else if (xx < 0) { xx += 32; if (0 < yy) yy--; else continue; }
+                                    pji = fma(g[yy][xx], up[i + 10], pji);
+                                }
+                                P += pji * exp(etols);
+                            }
+                        }
+                        nxt[y][t] = pji;
+                    }
+                memcpy(g, nxt, sizeof(nxt));
+                Pj = P;
+                sigma = sigma + Pj / (double)j;
+                mn += minu;
+                mx += maxu;
+            }
+            K = lambda * exp(-2.0 * sigma) / (H * (1.0 - exp(-lambda)));
+        }
+    }
+    out[0] = lambda;
+    out[1] = K;
+    out[2] = H;
+    out[3] = E;
+}
+
+/* ------------------------------------------------------------------------
  * Incomplete beta (log) and incomplete gamma (log of the upper tail), after
  * the published Cephes single-precision algorithms (incbetf: continued
  * fractions #1/#2 and power series; igamcf/igamf), as restated in

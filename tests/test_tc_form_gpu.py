@@ -124,3 +124,58 @@ def test_forms_dp_optima_and_evalues_against_fp64(ss_table):
     print("\nform    cell max-abs  DP optimum rel  phase-1 score rel  log E rel   (vs FP64 cells)")
     for name, (a, b, c, d) in report.items():
         print(f"{name:7s} {a:12.3e}  {b:14.3e}  {c:17.3e}  {d:10.3e}")
+
+
+def test_fp64_parameter_fit(oracle_lib, ss_table):
+    """The precision forms fit lambda, K and H of every passed pair in FP64
+    on the GPU and compute its E-value from them (the rest stays FP32).
+    Checked against the oracle's FP64 restatement of the fit on the same
+    histogram (relative 1e-9), the FP32 fit of the same run against the
+    oracle's FP32 fit (bit for bit), and each pair's log E-value against the
+    oracle's FP32 E-value computation fed the oracle's FP64 parameters. The
+    FP32 fit's relative error against FP64 is reported."""
+    import cother_b200 as cb
+    from cother_b200 import synth
+    O = oracle_lib
+    q = synth.make_profiles([160], 981, True)
+    db = synth.make_profiles(synth.lognormal_lengths(60, 160, 30, 400, seed=982), 983, False)
+    synth.plant_homologs(q, db, 0.2, seed=984)
+    o = cb.Options.defaults()
+    o.tc_form = cb.TC_BF16X3
+    with cb.BatchProcessing(ss_table, o) as bp:
+        bp.set_score_threshold(-1.0)            # every pair passes
+        bp.set_db_details(db.npositions * 100, db.nprofiles * 100)
+        bp.transfer_cpm_data(db)
+        bp.process_score_matrix(q)
+        sc, _, _ = bp.read_score_matrix(q.npositions, db.npositions)
+        recs = cb.records_table(bp.read_statistics())
+        fits = bp.read_fits()
+        sspace, _ = bp.search_space()
+    n = len(recs["score"])
+    assert n == db.nprofiles and fits.shape == (n, 8)
+    errs = {"lambda": 0.0, "K": 0.0, "H": 0.0}
+    nfit = 0
+    for k in range(n):
+        p = int(recs["org_pro_no"][k])
+        s0, Ld = int(db.starts[p]), int(db.lens[p])
+        st, cnt = O.pair_statistics(sc[:, s0:s0 + Ld], q.aa, db.aa[s0:s0 + Ld], recs["score"][k],
+                                    recs["psts"][k], q.npositions, Ld, q.eno[0], db.eno[p], sspace)
+        f64 = O.stat_params64(cnt)
+        # FP64 fit: the oracle's FP64 restatement
+        assert np.allclose(fits[k, :4], f64, rtol=1e-9, atol=1e-12), (p, fits[k, :4], f64)
+        # FP32 fit of the same run: the oracle's FP32 fit, bit for bit
+        assert np.array_equal(fits[k, 4:].astype(np.float32),
+                              np.array([st[8], st[9], st[7], st[6]], np.float32)), (p, fits[k, 4:], st)
+        # the E-value from the FP64 parameters
+        sig = O.significance(q.npositions, Ld, q.eno[0], db.eno[p], recs["score"][k], recs["psts"][k],
+                             np.float32(f64[0]), np.float32(f64[1]), sspace)
+        assert recs["log_evalue"][k] == sig[2], (p, recs["log_evalue"][k], sig[2])
+        assert recs["lambda"][k] == np.float32(f64[0]) and recs["K"][k] == np.float32(f64[1])
+        if f64[0] > 0 and f64[1] > 0:
+            nfit += 1
+            for name, i in (("lambda", 0), ("K", 1), ("H", 2)):
+                errs[name] = max(errs[name], abs(fits[k, 4 + i] - fits[k, i]) / abs(fits[k, i]))
+    assert nfit >= 10, nfit
+    assert errs["lambda"] < 1e-4 and errs["K"] < 1e-3 and errs["H"] < 1e-4, errs
+    print("\nFP32 parameter fit vs FP64 (%d pairs): max relative error lambda %.2e, K %.2e, H %.2e"
+          % (nfit, errs["lambda"], errs["K"], errs["H"]))
