@@ -84,7 +84,7 @@ def build_main(force: bool = False, verbose_ptxas: bool = False) -> str:
     if not force and _newer(LIB_MAIN, deps):
         return LIB_MAIN
     tmp = LIB_MAIN + ".tmp"
-    cmd = [_nvcc(), "-shared", "-o", tmp] + nvcc_flags(verbose_ptxas) + srcs + ["-lcublas", "-lpthread"]
+    cmd = [_nvcc(), "-shared", "-o", tmp] + nvcc_flags(verbose_ptxas) + srcs + ["-lpthread"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB_MAIN)
     return LIB_MAIN

@@ -198,8 +198,9 @@ struct cbp_context {
     float dmstab_h[kDstCard * kDstCard];
     DevBuf sstab, dmstab;
     // tensor-core form of the profile-profile term
-    cublasHandle_t cublas = nullptr;
-    DevBuf tcq_hi, tcq_lo, tcd_hi, tcd_lo;
+    DevBuf tcq;            // the query operand image of the tensor-core form
+    DevBuf tcerr;          // set by the tensor-core kernel when a wait gave up
+    int h_tcerr = 0;
     // the resident database chunk; contexts on one device may share it
     // (cbp_share_database), the last owner frees it
     std::shared_ptr<ProfilesStore> db = std::make_shared<ProfilesStore>();
@@ -448,7 +449,7 @@ size_t slab_bytes_per_position(const cbp_options& o, int Lq)
     const size_t nb = (size_t)map_bands(Lq);
     size_t b = (size_t)Lq * 9 + 172 + nb * (8 * 32 + 12) + 4 * kMapMaxWarps * kMapEdgeFields + 5 +
                (size_t)Lq * 5;
-    if (o.tc_form != CBP_TC_PLAIN) b += 2 * tc_operand_bytes(o.tc_form, 1);
+    (void)o;   // the tensor-core form needs only the query's operand image (per query, not per position)
     return b;
 }
 
@@ -631,6 +632,7 @@ int cbp_create(int device, const cbp_options* opt, const float* ss_table, size_t
             CBP_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
             for (auto& e : c->ev) CBP_CUDA(cudaEventCreate(&e));
             dp1_set_attributes();
+            tc_set_attributes();
             std::memcpy(c->sstab_h, ss_table, sizeof(c->sstab_h));
             build_dms_table(c->dmstab_h);
             c->nnweights.reserve(sizeof(kNNWeightsTable));
@@ -666,8 +668,7 @@ int cbp_destroy(cbp_context* c)
         b->release();
     c->sstab.release();
     c->dmstab.release();
-    for (DevBuf* b : {&c->tcq_hi, &c->tcq_lo, &c->tcd_hi, &c->tcd_lo}) b->release();
-    if (c->cublas) cublasDestroy(c->cublas);
+    for (DevBuf* b : {&c->tcq, &c->tcerr}) b->release();
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -917,15 +918,10 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             const bool tc = c->opt.tc_form != CBP_TC_PLAIN;
             if (tc) {
                 CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
-                if (!c->cublas) {
-                    if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS)
-                        throw Error(CBP_ERR_CUDA, "cuBLAS handle creation failed");
-                }
                 const int f = c->opt.tc_form;
-                c->tcq_hi.reserve(tc_operand_bytes(f, Lq));
-                c->tcq_lo.reserve(tc_operand_bytes(f, Lq));
-                c->tcd_hi.reserve(tc_operand_bytes(f, s.ncols));
-                c->tcd_lo.reserve(tc_operand_bytes(f, s.ncols));
+                c->tcq.reserve(tc_query_image_bytes(f, Lq));
+                c->tcerr.reserve(sizeof(int));
+                CBP_CUDA(cudaMemsetAsync(c->tcerr.p, 0, sizeof(int), c->stream));
                 TcArgs t;
                 t.q = a.q;
                 t.db = a.db;
@@ -933,11 +929,12 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
                 t.ncols = a.ncols;
                 t.ld = a.ld;
                 t.Lq = Lq;
-                tc_profile_sums(t, f, c->cublas, c->tcq_hi.p, c->tcq_lo.p, c->tcd_hi.p, c->tcd_lo.p,
-                                a.scores, c->stream);
+                const int nl = tc_profile_sums(t, f, c->tcq.p, a.scores, c->tcerr.as<int>(), c->stream);
+                CBP_CUDA(cudaMemcpyAsync(&c->h_tcerr, c->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost,
+                                         c->stream));
                 a.dots_in_scores = true;
-                c->launches += 2;   // the two operand-split kernels (the GEMMs are cuBLAS's)
-                c->stage_launches[0] += 2;
+                c->launches += nl;   // the query operand image and the tcgen05 contraction
+                c->stage_launches[0] += nl;
             }
 
             Dp1Args d;
@@ -1022,6 +1019,8 @@ int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* co
             CBP_CUDA(cudaStreamSynchronize(c->stream));
             if (c->h_dp1err)
                 throw Error(CBP_ERR_CUDA, "phase-1 DP: a wait for staged score rows timed out");
+            if (tc && c->h_tcerr)
+                throw Error(CBP_ERR_CUDA, "tensor-core contraction: a wait timed out");
             float ms = 0.f;
             CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
             c->stage_ms[0] += ms;

@@ -1,8 +1,8 @@
 // Tensor-core form of the profile-profile term: interface.
 #pragma once
 
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include "layout.h"
 
 namespace cbp {
@@ -16,12 +16,16 @@ struct TcArgs {
     int Lq = 0;
 };
 
-// bytes of one operand (high or low part) for `rows` positions
-size_t tc_operand_bytes(int form, long long rows);
+// bytes of the query operand image for a query of Lq positions
+size_t tc_query_image_bytes(int form, long long Lq);
 
-// The profile-profile sums of the slab into out ([Lq][ld]): operand
-// preparation kernels and three cuBLAS GEMMs on `stream`.
-void tc_profile_sums(const TcArgs& a, int form, cublasHandle_t h, void* qhi, void* qlo, void* dhi,
-                     void* dlo, float* out, cudaStream_t stream);
+// Per device, before the first tc_profile_sums (and outside any stream
+// capture): the shared-memory opt-in of the tensor-core kernel.
+void tc_set_attributes();
+
+// The profile-profile sums of the slab into out ([Lq][ld]) on `stream`:
+// the query operand image (qimg, tc_query_image_bytes) and the tcgen05
+// contraction; *err is set to 1 when a wait gave up. Returns the launches.
+int tc_profile_sums(const TcArgs& a, int form, void* qimg, float* out, int* err, cudaStream_t stream);
 
 }  // namespace cbp
