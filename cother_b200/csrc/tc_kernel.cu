@@ -15,9 +15,9 @@
 // one contraction of length 64: the database row is [hi | hi | lo | 0 0 0 0]
 // and the query row [hi | lo | hi | 0 0 0 0] (20 + 20 + 20 + 4).
 //
-// Kernel. Persistent CTAs of 128 threads walk tiles of 128 database
-// positions (the MMA's M: tensor-memory lanes) by up to 256 query rows (its
-// N: tensor-memory columns, FP32 accumulator). Per tile:
+// Kernel. Persistent CTAs of 128 threads (three or four per SM) walk tiles
+// of 128 database positions (the MMA's M: tensor-memory lanes) by up to 128
+// query rows (its N: tensor-memory columns, FP32 accumulator). Per tile:
 //  * the database rows are computed in the kernel from the resident
 //    frequencies and backgrounds (the split fused in; nothing of it goes
 //    through HBM) and stored in shared memory in the MMA's K-major
@@ -48,11 +48,10 @@ namespace cbp {
 namespace {
 
 constexpr int kTM = 128;                 // database positions per tile (MMA M)
-constexpr int kTNMax = 256;              // query rows per tile (MMA N, at most)
+constexpr int kTNMax = 128;              // query rows per tile (MMA N, at most)
 constexpr int kKE = 64;                  // contraction length (3 x 20 + 4 zeros)
 constexpr int kThreads = 128;
-constexpr int kTmemCols = 256;           // FP32 accumulator columns
-constexpr size_t kSmemRequest = 100 * 1024;   // caps residency at two CTAs per SM
+constexpr int kTmemCols = 128;           // FP32 accumulator columns (four CTAs fill the 512)
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
 template <bool kBf16> struct Form {
@@ -64,6 +63,11 @@ template <bool kBf16> struct Form {
     static constexpr uint32_t kFmt = kBf16 ? 1u : 2u;     // operand format: BF16 / TF32
     static constexpr int kABytes = kTM * kRowBytes;
     static constexpr int kBBytes = kTNMax * kRowBytes;
+    // dynamic shared memory requested per CTA: at most four CTAs per SM
+    // (BF16: 32 KB of tiles) or three (TF32: 64 KB), so that their tensor
+    // memory (128 columns each) always fits and no allocation waits
+    static constexpr size_t kSmemRequest = kBf16 ? 48 * 1024 : 64 * 1024;
+    static constexpr int kCtasPerSm = kBf16 ? 4 : 3;
 };
 
 // byte offset of 16-byte chunk kc of row r in the no-swizzle K-major layout
@@ -185,7 +189,7 @@ __device__ __forceinline__ void store_row(uint8_t* dst, const uint32_t* hi, cons
 }
 
 // The query operand as the shared-memory image of each query tile: tile t
-// (rows 256t..256t+255) at t * kBBytes; rows past the query are zero.
+// (rows 128t..128t+127) at t * kBBytes; rows past the query are zero.
 template <bool kBf16>
 __global__ void __launch_bounds__(128)
 tc_query_image_kernel(const TcArgs a, uint8_t* __restrict__ img, int ntiles)
@@ -314,20 +318,30 @@ tc_umma_kernel(const TcArgs a, const uint8_t* __restrict__ qimg, float* __restri
             // database positions, columns its query rows
             const long long col = m0 + 32 * warp + lane;
             const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
-            for (int j0 = 0; j0 < N; j0 += 16) {
-                uint32_t v[16];
+            for (int j0 = 0; j0 < N; j0 += 32) {
+                // two 16-column loads in flight per wait (N is a multiple of 16)
+                uint32_t v[32];
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
                              "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
                              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
                                "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
                                "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
                              : "r"(taddr + (uint32_t)j0));
+                const bool two = j0 + 16 < N;
+                if (two)
+                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                                 : "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                                   "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                                   "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                                 : "r"(taddr + (uint32_t)(j0 + 16)));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 if (col < a.ncols) {
+                    float* o = out + (long long)(n0 + j0) * a.ld + col;
 #pragma unroll
-                    for (int jj = 0; jj < 16; jj++) {
-                        const int r = n0 + j0 + jj;
-                        if (r < a.Lq) out[(long long)r * a.ld + col] = __uint_as_float(v[jj]);
+                    for (int jj = 0; jj < 32; jj++) {
+                        if (jj >= 16 && !two) break;
+                        if (n0 + j0 + jj < a.Lq) o[(long long)jj * a.ld] = __uint_as_float(v[jj]);
                     }
                 }
             }
@@ -359,9 +373,9 @@ int launch_form(const TcArgs& a, void* qimg, float* out, int* err, cudaStream_t 
         a, static_cast<uint8_t*>(qimg), ntiles);
     CBP_CHECK_LAUNCH();
     const int mtiles = (int)ceil_div(a.ncols, kTM);
-    const int grid = (int)std::min<long long>(mtiles, 2LL * sm_count());
-    tc_umma_kernel<kBf16><<<grid, kThreads, kSmemRequest, stream>>>(a, static_cast<const uint8_t*>(qimg), out,
-                                                                     err);
+    const int grid = (int)std::min<long long>(mtiles, (long long)Form<kBf16>::kCtasPerSm * sm_count());
+    tc_umma_kernel<kBf16><<<grid, kThreads, Form<kBf16>::kSmemRequest, stream>>>(
+        a, static_cast<const uint8_t*>(qimg), out, err);
     CBP_CHECK_LAUNCH();
     return 2;
 }
@@ -371,9 +385,9 @@ int launch_form(const TcArgs& a, void* qimg, float* out, int* err, cudaStream_t 
 void tc_set_attributes()
 {
     CBP_CUDA(cudaFuncSetAttribute(tc_umma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kSmemRequest));
+                                  (int)Form<true>::kSmemRequest));
     CBP_CUDA(cudaFuncSetAttribute(tc_umma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kSmemRequest));
+                                  (int)Form<false>::kSmemRequest));
 }
 
 size_t tc_query_image_bytes(int form, long long Lq)
