@@ -79,6 +79,8 @@ def load_library(path: str | None = None):
         "cbp_get_capacities": (i32, [vp, sz, sz] + [ctypes.POINTER(sz)] * 4),
         "cbp_transfer_chunk": (i32, [vp, vp, vp, vp]),
         "cbp_process": (i32, [vp, i32, sz, vp, vp]),
+        "cbp_process_batch": (i32, [vp, sz, vp, vp, vp]),
+        "cbp_select_query": (i32, [vp, sz, ctypes.POINTER(sz)]),
         "cbp_wait_idle": (i32, [vp]),
         "cbp_read_score_matrix": (i32, [vp, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
         "cbp_set_max_slab_positions": (i32, [vp, sz]),
@@ -275,6 +277,25 @@ class BatchProcessing:
         """Search one query profile against the resident chunk."""
         beg, end = query.field_tables()
         _check(load_library().cbp_process(self._h, int(query_serial), int(query.npositions), beg, end))
+
+    def process_batch(self, queries) -> None:
+        """Search several query profiles in one pass over the resident chunk
+        (cbp_process_batch); select_query(k) picks whose results the result
+        calls return (query 0 after the call)."""
+        n = len(queries)
+        tables = [q.field_tables() for q in queries]
+        lens = (ctypes.c_size_t * n)(*[q.npositions for q in queries])
+        beg = (ctypes.c_void_p * n)(*[ctypes.cast(t[0], ctypes.c_void_p) for t in tables])
+        end = (ctypes.c_void_p * n)(*[ctypes.cast(t[1], ctypes.c_void_p) for t in tables])
+        _check(load_library().cbp_process_batch(self._h, n, lens, beg, end))
+        self._batch = list(queries)
+
+    def select_query(self, k: int) -> int:
+        """Results of query k of the last call from now on; returns the
+        call's number of queries (cbp_select_query)."""
+        n = ctypes.c_size_t()
+        _check(load_library().cbp_select_query(self._h, int(k), ctypes.byref(n)))
+        return n.value
 
     def wait_idle(self) -> None:
         _check(load_library().cbp_wait_idle(self._h))

@@ -188,6 +188,20 @@ struct Tuning {
     float dp_ms[kDpCandidates] = {};
     long long sample_cols = 0;
 };
+// The results of one query of a cbp_process or cbp_process_batch call.
+struct QueryResult {
+    int Lq = 0;
+    int row0 = 0;                    // its first row in the (stacked) score matrix
+    float eno = 0.f;
+    float score_thld = 0.f, logE_thld = 0.f;
+    unsigned long long searchspace = 0;
+    size_t delta_length = 0;
+    std::vector<float> h_recs;       // hit records, all slabs
+    std::vector<char> h_alns[5];     // alignment rows, all slabs
+    std::vector<int32_t> h_order;    // reported hits in the finalizer's order (sorted on the device)
+    long long base_len = 0, base_npass = 0;   // running phase-2 offsets over slabs
+    long long last_npos2 = 0;
+};
 }  // namespace cbp
 
 struct cbp_context {
@@ -228,24 +242,22 @@ struct cbp_context {
     DevBuf hitrecs, statrecs, cs2, fb2, sg2, bt2, strip2, maperr, alnbuf, dp1err;
     DevBuf hitkeys, hitcnt;    // sort keys of all records of a query, reported count
     DevBuf fits;               // the precision forms: FP64 and FP32 parameter fits per passed pair
-    std::vector<int32_t> h_order;   // reported hits in the finalizer's order (sorted on the device)
-    std::vector<char> h_alns[5];
-    long long base_len = 0, base_npass = 0;   // running phase-2 offsets over slabs
-    long long last_npos2 = 0;
+    DevBuf qtrn;               // batches: each query's transitions as [7][Lq+1]
+
     int h_maperr = 0;   // set by the MAP stage when a wait between warps gave up
     int h_dp1err = 0;   // set by the phase-1 DP when a staging wait gave up
     bool score_thld_set = false, logE_thld_set = false;
     // results of the last process() call, all slabs
-    std::vector<float> h_recs;
-    unsigned long long searchspace = 0;
-    size_t delta_length = 0;
-    float query_eno = 0.f;
+    std::vector<QueryResult> res;   // per query of the last call
+    size_t cur = 0;                 // the query the result calls read (cbp_select_query)
     // last slab
     long long last_col0 = 0;
     int last_ncols = 0;
     long long last_ld = 0;
     int last_first_profile = 0;
     int last_Lq = 0;
+    long long last_row0 = 0;        // first score-matrix row of the inspected query
+    long long last_dp_off = 0;      // its slot in the phase-1 buffers (profiles)
     int last_nprof = 0;
     int last_npass = 0;
     // kernel variants chosen by the tuner, per query-length bin (Lq / 64)
@@ -465,6 +477,12 @@ size_t slab_fixed_bytes(int Lq)
 // logf as the reference does: dimension 19, kappa0 0.1, nu0 19;
 // 1/kappa0, -(nu0+2)/2 and (dim/2 - (nu0+2)/2) (ln kappa0 - ln(kappa0+2))
 // + sum_{i=1..dim} (ln(nu0+1-i) - ln 2).
+const QueryResult& cur_result(const cbp_context* c)
+{
+    static const QueryResult kNone;
+    return c->cur < c->res.size() ? c->res[c->cur] : kNone;
+}
+
 void cvs_constants(float* lokappa0, float* pownu0, float* cterm)
 {
     const int dim = 19;
@@ -579,6 +597,509 @@ void tune_kernels(cbp_context* c, const ScoreArgs& base, int p0, int p1, Tuning&
 
 }  // namespace
 
+namespace {
+
+// The field tables of nq single-profile queries as one profile set: each
+// field's bytes in query order (per-position and per-profile fields alike),
+// the profile offsets (pps2DDist) recomputed from the lengths. A field
+// missing from any query is left out.
+struct StackedTables {
+    std::vector<std::vector<char>> bytes;
+    char* beg[CBP_NFIELDS];
+    char* end[CBP_NFIELDS];
+};
+
+void stack_tables(size_t nq, char* const* const* qbeg, char* const* const* qend, StackedTables& t)
+{
+    t.bytes.assign(CBP_NFIELDS, {});
+    for (int f = 0; f < CBP_NFIELDS; f++) {
+        bool all = true;
+        size_t total = 0;
+        for (size_t k = 0; k < nq; k++) {
+            if (!qbeg[k] || !qend[k]) throw Error(CBP_ERR_ARG, "null field tables");
+            if (!qbeg[k][f] || !qend[k][f] || qend[k][f] < qbeg[k][f]) { all = false; break; }
+            total += (size_t)(qend[k][f] - qbeg[k][f]);
+        }
+        if (!all) { t.beg[f] = t.end[f] = nullptr; continue; }
+        std::vector<char>& v = t.bytes[f];
+        v.resize(std::max<size_t>(total, 1));
+        size_t off = 0;
+        for (size_t k = 0; k < nq; k++) {
+            const size_t n = (size_t)(qend[k][f] - qbeg[k][f]);
+            if (n) std::memcpy(v.data() + off, qbeg[k][f], n);
+            off += n;
+        }
+        t.beg[f] = v.data();
+        t.end[f] = v.data() + total;
+    }
+    if (!t.beg[fLen] || !t.beg[fDist] ||
+        (size_t)(t.end[fLen] - t.beg[fLen]) != nq * sizeof(int) ||
+        (size_t)(t.end[fDist] - t.beg[fDist]) != nq * sizeof(uint32_t))
+        throw Error(CBP_ERR_ARG, "each query's field tables must hold one profile");
+    const int* lens = reinterpret_cast<const int*>(t.beg[fLen]);
+    uint32_t* dist = reinterpret_cast<uint32_t*>(t.beg[fDist]);
+    uint32_t acc = 0;
+    for (size_t k = 0; k < nq; k++) {
+        dist[k] = acc;
+        acc += (uint32_t)lens[k];
+    }
+}
+
+// One search of nq queries against the resident chunk. The queries' rows
+// are stacked into one score matrix per slab (one column-order and one
+// score-kernel launch for all of them: one pass over the slab's database
+// columns); phase 1 of each query follows in the same CUDA graph, each on
+// its rows of the matrix and its own phase-1 buffers; statistics, MAP and
+// the hit order then run per query. With nq == 1 this is the search of one
+// query (CuBatchProcessing::ProcessScoreMatrix).
+void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const* const* qbeg,
+                     char* const* const* qend)
+{
+    check_ctx(c);
+    if (!c->have_db) throw Error(CBP_ERR_STATE, "no database chunk transferred");
+    if (nq == 0) throw Error(CBP_ERR_ARG, "no query");
+    if (c->opt.cvswgt > 0.0f) {
+        if (!c->have_cvs)
+            throw Error(CBP_ERR_STATE, "CVSWGT > 0 needs the context-vector map (cbp_set_cvs2s_map)");
+        if (!c->db->view.cv)
+            throw Error(CBP_ERR_STATE, "CVSWGT > 0 needs a database chunk with context vectors "
+                                       "(transferred by a context with CVSWGT > 0)");
+    }
+    if (nq == 1) {
+        upload_profiles(c->query, qbeg[0], qend[0], c->stream, c->opt.cvswgt > 0.0f);
+        if (c->query.view.P != 1) throw Error(CBP_ERR_ARG, "the query field tables must hold one profile");
+    } else {
+        StackedTables t;
+        stack_tables(nq, qbeg, qend, t);
+        upload_profiles(c->query, t.beg, t.end, c->stream, c->opt.cvswgt > 0.0f);
+    }
+    const int Ltot = (int)c->query.view.N;
+    std::vector<QueryResult> res(nq);
+    {
+        long long row = 0;
+        for (size_t k = 0; k < nq; k++) {
+            if ((size_t)c->query.h_plen[k] != qlens[k])
+                throw Error(CBP_ERR_ARG, "query_len differs from the query profile length");
+            QueryResult& r = res[k];
+            r.Lq = (int)qlens[k];
+            r.row0 = (int)row;
+            r.eno = c->query.h_eno[k];
+            row += r.Lq;
+            // effective search space (AbstractScoreMatrix::ComputeLengthAdjustment);
+            // the query length and the database totals default to this
+            // query and this chunk when not set
+            const size_t m = (nq == 1 && c->query_len) ? c->query_len : (size_t)r.Lq;
+            const unsigned long long n = c->db_len ? c->db_len : (unsigned long long)c->db->view.N;
+            const size_t N = c->n_seqs ? c->n_seqs : (size_t)c->db->view.P;
+            length_adjustment(c->gap_lambda, c->gap_K, c->gap_alpha, c->gap_beta, m, n, N, &r.searchspace,
+                              &r.delta_length);
+            // thresholds not set by the caller follow from EVAL as the
+            // reference's job dispatcher derives them
+            float sthld = 0.f, lthld = 0.f;
+            cbp_score_threshold(m, n, c->opt.eval, c->gap_lambda, c->gap_K, &sthld, &lthld);
+            r.score_thld = c->score_thld_set ? c->score_thld : sthld;
+            r.logE_thld = c->logE_thld_set ? c->logE_thld : lthld;
+        }
+    }
+    c->launches = 0;
+    for (float& m : c->stage_ms) m = 0.f;
+    for (uint64_t& m : c->stage_launches) m = 0;
+    c->res.clear();
+    c->cur = 0;
+
+    std::vector<Slab> slabs = plan_slabs(c, Ltot);
+    size_t maxcols = 0, maxprof = 0;
+    for (const Slab& s : slabs) {
+        maxcols = std::max(maxcols, (size_t)align_up(s.ncols, 32));
+        maxprof = std::max(maxprof, (size_t)(s.p1 - s.p0));
+    }
+    const size_t keycap = (size_t)hit_sort_capacity(c->db->view.P);
+    c->scores.reserve((size_t)Ltot * maxcols * sizeof(float));
+    c->modscores.reserve((size_t)Ltot * maxcols * sizeof(float));
+    c->btck.reserve((size_t)Ltot * maxcols);
+    c->bandbuf.reserve(5 * maxcols * sizeof(float));
+    c->colorder.reserve(maxcols * sizeof(int));
+    c->dpmax.reserve(nq * maxprof * sizeof(float));
+    c->dpcoords.reserve(nq * maxprof * sizeof(uint32_t));
+    c->dprecs.reserve(nq * maxprof * sizeof(Dp1Rec));
+    c->passidx.reserve(nq * maxprof * sizeof(int));
+    c->passdst.reserve(nq * maxprof * sizeof(long long));
+    c->passcnt.reserve(nq * 16);
+    c->dp1err.reserve(sizeof(int));
+    c->hitkeys.reserve(nq * keycap * sizeof(uint64_t));
+    c->hitcnt.reserve(nq * sizeof(int));
+    CBP_CUDA(cudaMemsetAsync(c->hitcnt.p, 0, nq * sizeof(int), c->stream));
+    // each query's transitions as the kernels index them ([7][Lq+1])
+    std::vector<const float*> qtrn(nq, c->query.view.trn);
+    if (nq > 1) {
+        size_t tot = 0;
+        for (const QueryResult& r : res) tot += (size_t)kNTrn * (r.Lq + 1);
+        c->qtrn.reserve(tot * sizeof(float));
+        const long long NT = c->query.view.N + c->query.view.P;
+        size_t off = 0;
+        for (size_t k = 0; k < nq; k++) {
+            const QueryResult& r = res[k];
+            float* dst = c->qtrn.as<float>() + off;
+            CBP_CUDA(cudaMemcpy2DAsync(dst, (size_t)(r.Lq + 1) * sizeof(float),
+                                       c->query.view.trn + r.row0 + (long long)k, (size_t)NT * sizeof(float),
+                                       (size_t)(r.Lq + 1) * sizeof(float), kNTrn, cudaMemcpyDeviceToDevice,
+                                       c->stream));
+            qtrn[k] = dst;
+            off += (size_t)kNTrn * (r.Lq + 1);
+        }
+    }
+    const bool tc = c->opt.tc_form != CBP_TC_PLAIN;
+
+    for (const Slab& s : slabs) {
+        ScoreArgs a;
+        a.q = c->query.view;
+        a.db = c->db->view;
+        a.col0 = s.col0;
+        a.ncols = s.ncols;
+        a.ld = align_up(s.ncols, 32);
+        a.Lq = Ltot;
+        a.ssswgt = c->opt.ssswgt;
+        a.ddmswgt = c->opt.ddmswgt;
+        a.initshift = c->opt.mapaln ? 0.002f : 0.0003f;
+        a.dstsegm = c->opt.dstsegm;
+        if (c->opt.cvswgt > 0.0f) {
+            a.cvswgt = c->opt.cvswgt;
+            a.cvs_scores = c->cvsmap.as<float>();
+            a.cvs_card = c->cvs_card;
+            a.cvs_shift = c->cvs_shift;
+            a.cvs_key_first = c->cvs_key_first;
+            a.cvs_key_last = c->cvs_key_last;
+            cvs_constants(&a.cvs_lokappa0, &a.cvs_pownu0, &a.cvs_cterm);
+            a.cvs_int_priors = !c->opt.mapaln;
+        }
+        a.sstab = c->sstab.as<float>();
+        a.dmstab = c->dmstab.as<float>();
+        a.scores = c->scores.as<float>();
+        a.modscores = c->modscores.as<float>();
+        a.colorder = c->colorder.as<int>();
+        Tuning& tn = c->tuning[Ltot / 64];
+        if (c->opt.autotune && !tn.tuned) tune_kernels(c, a, s.p0, s.p1, tn);
+        a.rows = tn.rows;
+        if (tc) {
+            // the profile-profile sums on the tensor cores, per query (its
+            // database operand depends on the query's background)
+            CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
+            const int f = c->opt.tc_form;
+            size_t img = 0;
+            for (const QueryResult& r : res) img = std::max(img, tc_query_image_bytes(f, r.Lq));
+            c->tcq.reserve(img);
+            c->tcerr.reserve(sizeof(int));
+            CBP_CUDA(cudaMemsetAsync(c->tcerr.p, 0, sizeof(int), c->stream));
+            for (size_t k = 0; k < nq; k++) {
+                TcArgs t;
+                t.q = a.q;
+                t.db = a.db;
+                t.col0 = a.col0;
+                t.ncols = a.ncols;
+                t.ld = a.ld;
+                t.Lq = res[k].Lq;
+                t.qrow0 = res[k].row0;
+                t.qprof = (int)k;
+                const int nl = tc_profile_sums(t, f, c->tcq.p, a.scores + (long long)res[k].row0 * a.ld,
+                                               c->tcerr.as<int>(), c->stream);
+                c->launches += nl;   // the query operand image and the tcgen05 contraction
+                c->stage_launches[0] += nl;
+            }
+            CBP_CUDA(cudaMemcpyAsync(&c->h_tcerr, c->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost,
+                                     c->stream));
+            a.dots_in_scores = true;
+        }
+
+        std::vector<Dp1Args> d(nq);
+        for (size_t k = 0; k < nq; k++) {
+            const QueryResult& r = res[k];
+            d[k].scores = a.scores + (long long)r.row0 * a.ld;
+            d[k].ld = a.ld;
+            d[k].Lq = r.Lq;
+            d[k].qtrn = qtrn[k];
+            d[k].db = c->db->view;
+            d[k].col0 = s.col0;
+            d[k].p0 = s.p0;
+            d[k].nprof = s.p1 - s.p0;
+            d[k].btck = c->btck.as<uint8_t>() + (long long)r.row0 * a.ld;
+            d[k].bandbuf = c->bandbuf.as<float>();
+            d[k].maxsc = c->dpmax.as<float>() + k * maxprof;
+            d[k].maxcoords = c->dpcoords.as<uint32_t>() + k * maxprof;
+            d[k].recs = c->dprecs.as<Dp1Rec>() + k * maxprof;
+            d[k].warps = tn.dp_warps;
+            d[k].err = c->dp1err.as<int>();
+        }
+        auto pass_idx = [&](size_t k) { return c->passidx.as<int>() + k * maxprof; };
+        auto pass_dst = [&](size_t k) { return c->passdst.as<long long>() + k * maxprof; };
+        auto pass_cnt = [&](size_t k) { return reinterpret_cast<int*>(c->passcnt.as<char>() + 16 * k); };
+        auto pass_npos = [&](size_t k) { return reinterpret_cast<long long*>(c->passcnt.as<char>() + 16 * k + 8); };
+
+        // phase 1 of the slab: column order, score matrix (all queries' rows),
+        // each query's DP, finalization and pass list; with the plain form
+        // one CUDA graph, captured here and swapped into the context's
+        // executable graph by an update of its parameters
+        auto phase1 = [&](bool capturing) {
+            auto mark = [&](cudaEvent_t e) {
+                if (capturing) CBP_CUDA(cudaEventRecordWithFlags(e, c->stream, cudaEventRecordExternal));
+                else CBP_CUDA(cudaEventRecord(e, c->stream));
+            };
+            if (!tc) mark(c->ev[0]);
+            launch_column_order(c->db->view.dstlen, s.col0, s.ncols, a.ld, tn.window, c->colorder.as<int>(),
+                                c->stream);
+            launch_score_matrix(a, c->stream);
+            mark(c->ev[1]);
+            CBP_CUDA(cudaMemsetAsync(c->dp1err.p, 0, sizeof(int), c->stream));
+            for (size_t k = 0; k < nq; k++) launch_dp1(d[k], c->stream);
+            mark(c->ev[2]);
+            for (size_t k = 0; k < nq; k++) {
+                launch_dp1_finalize(d[k], res[k].score_thld, c->stream);
+                launch_pass_compact(d[k], pass_idx(k), pass_dst(k), pass_cnt(k), pass_npos(k), c->stream);
+            }
+            mark(c->ev[3]);
+        };
+        if (tc) {
+            phase1(false);
+        } else {
+            CBP_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            cudaGraph_t g = nullptr;
+            try {
+                phase1(true);
+            } catch (...) {
+                cudaStreamEndCapture(c->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            CBP_CUDA(cudaStreamEndCapture(c->stream, &g));
+            if (c->phase1_exec) {
+                cudaGraphExecUpdateResultInfo info;
+                if (cudaGraphExecUpdate(c->phase1_exec, g, &info) != cudaSuccess) {
+                    (void)cudaGetLastError();
+                    cudaGraphExecDestroy(c->phase1_exec);
+                    c->phase1_exec = nullptr;
+                }
+            }
+            if (!c->phase1_exec) {
+                const cudaError_t e = cudaGraphInstantiate(&c->phase1_exec, g, 0);
+                if (e != cudaSuccess) {
+                    cudaGraphDestroy(g);
+                    c->phase1_exec = nullptr;
+                    CBP_CUDA(e);
+                }
+            }
+            cudaGraphDestroy(g);
+            CBP_CUDA(cudaGraphLaunch(c->phase1_exec, c->stream));
+            c->graph_launches += 1;
+        }
+        c->launches += 2 + 3 * (uint64_t)nq;
+        c->stage_launches[0] += 2;
+        c->stage_launches[1] += nq;
+        c->stage_launches[2] += 2 * (uint64_t)nq;
+        std::vector<int> npass(nq, 0);
+        for (size_t k = 0; k < nq; k++)
+            CBP_CUDA(cudaMemcpyAsync(&npass[k], pass_cnt(k), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CBP_CUDA(cudaMemcpyAsync(&c->h_dp1err, c->dp1err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CBP_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->h_dp1err)
+            throw Error(CBP_ERR_CUDA, "phase-1 DP: a wait for staged score rows timed out");
+        if (tc && c->h_tcerr)
+            throw Error(CBP_ERR_CUDA, "tensor-core contraction: a wait timed out");
+        float ms = 0.f;
+        CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+        c->stage_ms[0] += ms;
+        CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]));
+        c->stage_ms[1] += ms;
+        CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+        c->stage_ms[2] += ms;
+        // the inspection calls (cbp_read_*) see the last query of the slab
+        c->last_col0 = s.col0;
+        c->last_ncols = s.ncols;
+        c->last_ld = a.ld;
+        c->last_first_profile = s.p0;
+        c->last_Lq = res[nq - 1].Lq;
+        c->last_row0 = res[nq - 1].row0;
+        c->last_dp_off = (long long)(nq - 1) * (long long)maxprof;
+        c->last_nprof = s.p1 - s.p0;
+        c->last_npass = npass[nq - 1];
+
+        for (size_t k = 0; k < nq; k++) {
+            QueryResult& r = res[k];
+            const int np = npass[k];
+            if (np <= 0) continue;
+            const int Lq = r.Lq;
+            const float* sc = a.scores + (long long)r.row0 * a.ld;
+            // statistics and E-values of the passed pairs of this slab
+            c->hitrecs.reserve((size_t)np * kRecFloats * sizeof(float));
+            StatsArgs st;
+            st.scores = sc;
+            st.ld = a.ld;
+            st.Lq = Lq;
+            st.col0 = s.col0;
+            st.p0 = s.p0;
+            st.db = c->db->view;
+            st.qaa = c->query.view.aa + r.row0;
+            st.qeno = r.eno;
+            st.x_uninf = c->opt.x_uninf;
+            st.pass_idx = pass_idx(k);
+            st.pass_dst = pass_dst(k);
+            st.recs = d[k].recs;
+            st.out = c->hitrecs.as<float>();
+            st.nnweights = c->nnweights.as<float>();
+            st.ssemodel = c->opt.ssemodel;
+            st.searchspace = (float)r.searchspace;
+            st.ref_lambda = c->ref_lambda;
+            st.ref_K = c->ref_K;
+            st.exp_gapped_lambda = c->gap_lambda;
+            st.exp_gapped_K = c->gap_K;
+            if (tc) {
+                // the precision forms fit lambda, K, H in FP64 for the E-values
+                c->fits.reserve((size_t)np * kFitDoubles * sizeof(double));
+                st.fits = c->fits.as<double>();
+                st.use_fit64 = 1;
+            }
+            CBP_CUDA(cudaEventRecord(c->ev[4], c->stream));
+            launch_stats(st, np, c->stream);
+            CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
+            // the records as the statistics leave them (cbp_read_statistics)
+            c->statrecs.reserve((size_t)np * kRecFloats * sizeof(float));
+            CBP_CUDA(cudaMemcpyAsync(c->statrecs.p, c->hitrecs.p, (size_t)np * kRecFloats * sizeof(float),
+                                     cudaMemcpyDeviceToDevice, c->stream));
+            c->launches += 1;
+            c->stage_launches[3] += 1;
+
+            // phase-2 MAP realignment of the pairs within the E-value
+            // threshold (in the phase-2 column space of this slab)
+            long long npos2 = 0;
+            CBP_CUDA(cudaMemcpyAsync(&npos2, pass_npos(k), sizeof(long long), cudaMemcpyDeviceToHost,
+                                     c->stream));
+            CBP_CUDA(cudaStreamSynchronize(c->stream));
+            const long long nd = map_diag_rows(npos2);
+            const size_t nb = (size_t)map_bands(Lq);
+            const long long alnstride = align_up(npos2 + (long long)np * Lq, 32);
+            c->alnbuf.reserve(5 * (size_t)alnstride);
+            MapArgs mp;
+            mp.scores = sc;
+            mp.modscores = a.modscores + (long long)r.row0 * a.ld;
+            mp.ld = a.ld;
+            mp.Lq = Lq;
+            mp.col0 = s.col0;
+            mp.p0 = s.p0;
+            mp.db = c->db->view;
+            mp.qtrn = qtrn[k];
+            mp.qaa = c->query.view.aa + r.row0;
+            mp.qsss = c->query.view.sss + r.row0;
+            mp.printsss = c->opt.ssswgt > 0.0f;
+            mp.modscores_inuse = (c->opt.ssswgt > 0.0f || c->opt.cvswgt > 0.0f) ? 1 : 0;
+            mp.minpp = c->opt.minpp;
+            mp.logevthld = r.logE_thld;
+            mp.npass = np;
+            mp.pass_idx = pass_idx(k);
+            mp.pass_dst = pass_dst(k);
+            mp.recs = c->hitrecs.as<float>();
+            mp.alns = c->alnbuf.as<char>();
+            mp.alnstride = alnstride;
+            CBP_CUDA(cudaMemsetAsync(c->alnbuf.p, 0, 5 * (size_t)alnstride, c->stream));
+            if (c->opt.mapaln) {
+                c->cs2.reserve(nb * nd * 32 * sizeof(float));
+                c->fb2.reserve(nb * nd * 32 * sizeof(float));
+                c->sg2.reserve(nb * nd * sizeof(unsigned));
+                c->bt2.reserve(nb * nd * sizeof(unsigned long long));
+                c->strip2.reserve((size_t)map_strip_floats(npos2) * sizeof(float));
+                c->maperr.reserve(sizeof(int));
+                mp.nd = nd;
+                mp.cs = c->cs2.as<float>();
+                mp.fb = c->fb2.as<float>();
+                mp.sg = c->sg2.as<unsigned>();
+                mp.bt = c->bt2.as<unsigned long long>();
+                mp.strip = c->strip2.as<float>();
+                mp.err = c->maperr.as<int>();
+                CBP_CUDA(cudaMemsetAsync(c->maperr.p, 0, sizeof(int), c->stream));
+                CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
+                launch_map(mp, c->stream);
+                CBP_CUDA(cudaEventRecord(c->ev[7], c->stream));
+                CBP_CUDA(cudaMemcpyAsync(&c->h_maperr, c->maperr.p, sizeof(int), cudaMemcpyDeviceToHost,
+                                         c->stream));
+                c->launches += 2;
+                c->stage_launches[4] += 2;
+            } else {
+                // MAPALN=0: the phase-1 alignments themselves
+                // (CuBatchDP::FinalizeALNDynProgDevice)
+                CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
+                launch_aln_final(mp, d[k].btck, d[k].maxsc, d[k].maxcoords, c->stream);
+                CBP_CUDA(cudaEventRecord(c->ev[7], c->stream));
+                c->launches += 1;
+                c->stage_launches[4] += 1;
+            }
+            r.last_npos2 = npos2;
+            // sort keys of this slab's records, for the hit order
+            c->launches += launch_hit_keys(c->hitrecs.as<float>(), np, r.logE_thld, r.base_npass,
+                                           c->hitkeys.as<uint64_t>() + k * keycap, c->hitcnt.as<int>() + k,
+                                           c->stream);
+            c->stage_launches[5] += 1;
+            const size_t off = r.h_recs.size();
+            r.h_recs.resize(off + (size_t)np * kRecFloats);
+            CBP_CUDA(cudaMemcpyAsync(r.h_recs.data() + off, c->hitrecs.p, (size_t)np * kRecFloats * sizeof(float),
+                                     cudaMemcpyDeviceToHost, c->stream));
+            // this slab's alignment rows go to the running offset of
+            // the whole result (slot of pair K at newDst + K*Lq)
+            const long long shift = r.base_len + r.base_npass * (long long)Lq;
+            const long long slablen = npos2 + (long long)np * Lq;
+            for (int row = 0; row < 5; row++) {
+                r.h_alns[row].resize((size_t)(shift + slablen), 0);
+                CBP_CUDA(cudaMemcpyAsync(r.h_alns[row].data() + shift, c->alnbuf.as<char>() + (size_t)row * alnstride,
+                                         (size_t)slablen, cudaMemcpyDeviceToHost, c->stream));
+            }
+            CBP_CUDA(cudaStreamSynchronize(c->stream));
+            if (c->opt.mapaln && c->h_maperr)
+                throw Error(CBP_ERR_CUDA, "MAP realignment: a wait between the warps of a pair timed out");
+            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+            c->stage_ms[3] += ms;
+            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]));
+            c->stage_ms[4] += ms;
+            // phase-2 offsets of this slab's pairs become offsets in the
+            // whole result
+            for (size_t i = off; i < r.h_recs.size(); i += kRecFloats) {
+                uint32_t v;
+                std::memcpy(&v, &r.h_recs[i + rProNewDst], 4);
+                v += (uint32_t)r.base_len;
+                std::memcpy(&r.h_recs[i + rProNewDst], &v, 4);
+            }
+            r.base_len += npos2;
+            r.base_npass += np;
+        }
+    }
+    // the reported hits of each query in the finalizer's order: one sort
+    // over the keys of all its records; the reported ones come first
+    for (size_t k = 0; k < nq; k++) {
+        QueryResult& r = res[k];
+        if (r.base_npass <= 0) continue;
+        uint64_t* keys_d = c->hitkeys.as<uint64_t>() + k * keycap;
+        CBP_CUDA(cudaEventRecord(c->ev[4], c->stream));
+        const int nl = launch_hit_sort(keys_d, r.base_npass, c->stream);
+        CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
+        c->launches += nl;
+        c->stage_launches[5] += nl;
+        int nrep = 0;
+        CBP_CUDA(cudaMemcpyAsync(&nrep, c->hitcnt.as<int>() + k, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CBP_CUDA(cudaStreamSynchronize(c->stream));
+        if (nrep < 0 || nrep > r.base_npass) throw Error(CBP_ERR_CUDA, "hit order: inconsistent count");
+        std::vector<uint64_t> keys((size_t)nrep);
+        if (nrep > 0)
+            CBP_CUDA(cudaMemcpyAsync(keys.data(), keys_d, (size_t)nrep * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                     c->stream));
+        CBP_CUDA(cudaStreamSynchronize(c->stream));
+        r.h_order.resize((size_t)nrep);
+        for (int i = 0; i < nrep; i++) r.h_order[i] = (int32_t)(uint32_t)keys[i];
+        float ms = 0.f;
+        CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+        c->stage_ms[5] += ms;
+    }
+    CBP_CUDA(cudaStreamSynchronize(c->stream));
+    c->res = std::move(res);
+    c->cur = 0;
+}
+
+}  // namespace
+
 extern "C" {
 
 void cbp_default_options(cbp_options* o)
@@ -664,7 +1185,7 @@ int cbp_destroy(cbp_context* c)
     for (DevBuf* b : {&c->scores, &c->modscores, &c->btck, &c->bandbuf, &c->colorder, &c->dpmax, &c->dpcoords,
                       &c->dprecs, &c->passidx, &c->passdst, &c->passcnt, &c->hitrecs, &c->nnweights,
                       &c->cs2, &c->fb2, &c->sg2, &c->bt2, &c->strip2, &c->maperr, &c->alnbuf,
-                      &c->cvsmap, &c->statrecs, &c->dp1err, &c->hitkeys, &c->hitcnt, &c->fits})
+                      &c->cvsmap, &c->statrecs, &c->dp1err, &c->hitkeys, &c->hitcnt, &c->fits, &c->qtrn})
         b->release();
     c->sstab.release();
     c->dmstab.release();
@@ -822,389 +1343,25 @@ int cbp_set_cvs2s_map(cbp_context* c, const float* keys, const float* scores, si
 int cbp_process(cbp_context* c, int /*query_serial*/, size_t query_len, char* const* qbeg,
                 char* const* qend)
 {
+    return guarded([&] { process_queries(c, 1, &query_len, &qbeg, &qend); });
+}
+
+int cbp_process_batch(cbp_context* c, size_t nqueries, const size_t* query_lens, char* const* const* qbeg,
+                      char* const* const* qend)
+{
+    return guarded([&] {
+        if (!query_lens || !qbeg || !qend) throw Error(CBP_ERR_ARG, "null query arrays");
+        process_queries(c, nqueries, query_lens, qbeg, qend);
+    });
+}
+
+int cbp_select_query(cbp_context* c, size_t k, size_t* nqueries)
+{
     return guarded([&] {
         check_ctx(c);
-        if (!c->have_db) throw Error(CBP_ERR_STATE, "no database chunk transferred");
-        if (c->opt.cvswgt > 0.0f) {
-            if (!c->have_cvs)
-                throw Error(CBP_ERR_STATE, "CVSWGT > 0 needs the context-vector map (cbp_set_cvs2s_map)");
-            if (!c->db->view.cv)
-                throw Error(CBP_ERR_STATE, "CVSWGT > 0 needs a database chunk with context vectors "
-                                           "(transferred by a context with CVSWGT > 0)");
-        }
-        upload_profiles(c->query, qbeg, qend, c->stream, c->opt.cvswgt > 0.0f);
-        const int Lq = (int)c->query.view.N;
-        if (c->query.view.P != 1) throw Error(CBP_ERR_ARG, "the query field tables must hold one profile");
-        if ((size_t)Lq != query_len) throw Error(CBP_ERR_ARG, "query_len differs from the query profile length");
-        c->launches = 0;
-        for (float& m : c->stage_ms) m = 0.f;
-        for (uint64_t& m : c->stage_launches) m = 0;
-        c->h_recs.clear();
-        c->h_order.clear();
-        for (auto& r : c->h_alns) r.clear();
-        c->base_len = 0;
-        c->base_npass = 0;
-        c->last_npos2 = 0;
-        c->query_eno = *reinterpret_cast<const float*>(qbeg[fENO]);
-        {
-            // effective search space (AbstractScoreMatrix::ComputeLengthAdjustment);
-            // the query length and the database totals default to this
-            // query and this chunk when not set
-            const size_t m = c->query_len ? c->query_len : (size_t)Lq;
-            const unsigned long long n = c->db_len ? c->db_len : (unsigned long long)c->db->view.N;
-            const size_t N = c->n_seqs ? c->n_seqs : (size_t)c->db->view.P;
-            length_adjustment(c->gap_lambda, c->gap_K, c->gap_alpha, c->gap_beta, m, n, N,
-                              &c->searchspace, &c->delta_length);
-            // thresholds not set by the caller follow from EVAL as the
-            // reference's job dispatcher derives them
-            float sthld = 0.f, lthld = 0.f;
-            cbp_score_threshold(m, n, c->opt.eval, c->gap_lambda, c->gap_K, &sthld, &lthld);
-            if (!c->score_thld_set) c->score_thld = sthld;
-            if (!c->logE_thld_set) c->logE_thld = lthld;
-        }
-
-        std::vector<Slab> slabs = plan_slabs(c, Lq);
-        size_t maxcols = 0, maxprof = 0;
-        for (const Slab& s : slabs) {
-            maxcols = std::max(maxcols, (size_t)align_up(s.ncols, 32));
-            maxprof = std::max(maxprof, (size_t)(s.p1 - s.p0));
-        }
-        c->scores.reserve((size_t)Lq * maxcols * sizeof(float));
-        c->modscores.reserve((size_t)Lq * maxcols * sizeof(float));
-        c->btck.reserve((size_t)Lq * maxcols);
-        c->bandbuf.reserve(5 * maxcols * sizeof(float));
-        c->colorder.reserve(maxcols * sizeof(int));
-        c->dpmax.reserve(maxprof * sizeof(float));
-        c->dpcoords.reserve(maxprof * sizeof(uint32_t));
-        c->dprecs.reserve(maxprof * sizeof(Dp1Rec));
-        c->passidx.reserve(maxprof * sizeof(int));
-        c->passdst.reserve(maxprof * sizeof(long long));
-        c->passcnt.reserve(64);
-        c->dp1err.reserve(sizeof(int));
-        c->hitkeys.reserve((size_t)hit_sort_capacity(c->db->view.P) * sizeof(uint64_t));
-        c->hitcnt.reserve(sizeof(int));
-        CBP_CUDA(cudaMemsetAsync(c->hitcnt.p, 0, sizeof(int), c->stream));
-
-        for (const Slab& s : slabs) {
-            ScoreArgs a;
-            a.q = c->query.view;
-            a.db = c->db->view;
-            a.col0 = s.col0;
-            a.ncols = s.ncols;
-            a.ld = align_up(s.ncols, 32);
-            a.Lq = Lq;
-            a.ssswgt = c->opt.ssswgt;
-            a.ddmswgt = c->opt.ddmswgt;
-            a.initshift = c->opt.mapaln ? 0.002f : 0.0003f;
-            a.dstsegm = c->opt.dstsegm;
-            if (c->opt.cvswgt > 0.0f) {
-                a.cvswgt = c->opt.cvswgt;
-                a.cvs_scores = c->cvsmap.as<float>();
-                a.cvs_card = c->cvs_card;
-                a.cvs_shift = c->cvs_shift;
-                a.cvs_key_first = c->cvs_key_first;
-                a.cvs_key_last = c->cvs_key_last;
-                cvs_constants(&a.cvs_lokappa0, &a.cvs_pownu0, &a.cvs_cterm);
-                a.cvs_int_priors = !c->opt.mapaln;
-            }
-            a.sstab = c->sstab.as<float>();
-            a.dmstab = c->dmstab.as<float>();
-            a.scores = c->scores.as<float>();
-            a.modscores = c->modscores.as<float>();
-            a.colorder = c->colorder.as<int>();
-            Tuning& tn = c->tuning[Lq / 64];
-            if (c->opt.autotune && !tn.tuned) tune_kernels(c, a, s.p0, s.p1, tn);
-            a.rows = tn.rows;
-            const bool tc = c->opt.tc_form != CBP_TC_PLAIN;
-            if (tc) {
-                CBP_CUDA(cudaEventRecord(c->ev[0], c->stream));
-                const int f = c->opt.tc_form;
-                c->tcq.reserve(tc_query_image_bytes(f, Lq));
-                c->tcerr.reserve(sizeof(int));
-                CBP_CUDA(cudaMemsetAsync(c->tcerr.p, 0, sizeof(int), c->stream));
-                TcArgs t;
-                t.q = a.q;
-                t.db = a.db;
-                t.col0 = a.col0;
-                t.ncols = a.ncols;
-                t.ld = a.ld;
-                t.Lq = Lq;
-                const int nl = tc_profile_sums(t, f, c->tcq.p, a.scores, c->tcerr.as<int>(), c->stream);
-                CBP_CUDA(cudaMemcpyAsync(&c->h_tcerr, c->tcerr.p, sizeof(int), cudaMemcpyDeviceToHost,
-                                         c->stream));
-                a.dots_in_scores = true;
-                c->launches += nl;   // the query operand image and the tcgen05 contraction
-                c->stage_launches[0] += nl;
-            }
-
-            Dp1Args d;
-            d.scores = a.scores;
-            d.ld = a.ld;
-            d.Lq = Lq;
-            d.qtrn = c->query.view.trn;
-            d.db = c->db->view;
-            d.col0 = s.col0;
-            d.p0 = s.p0;
-            d.nprof = s.p1 - s.p0;
-            d.btck = c->btck.as<uint8_t>();
-            d.bandbuf = c->bandbuf.as<float>();
-            d.maxsc = c->dpmax.as<float>();
-            d.maxcoords = c->dpcoords.as<uint32_t>();
-            d.recs = c->dprecs.as<Dp1Rec>();
-            d.warps = tn.dp_warps;
-            d.err = c->dp1err.as<int>();
-
-            // phase 1 of the slab: column order, score matrix, DP, its
-            // finalization and the pass list; with the plain form one CUDA
-            // graph, captured here and swapped into the context's executable
-            // graph by an update of its parameters
-            auto phase1 = [&](bool capturing) {
-                auto mark = [&](cudaEvent_t e) {
-                    if (capturing) CBP_CUDA(cudaEventRecordWithFlags(e, c->stream, cudaEventRecordExternal));
-                    else CBP_CUDA(cudaEventRecord(e, c->stream));
-                };
-                if (!tc) mark(c->ev[0]);
-                launch_column_order(c->db->view.dstlen, s.col0, s.ncols, a.ld, tn.window, c->colorder.as<int>(),
-                                    c->stream);
-                launch_score_matrix(a, c->stream);
-                mark(c->ev[1]);
-                CBP_CUDA(cudaMemsetAsync(c->dp1err.p, 0, sizeof(int), c->stream));
-                launch_dp1(d, c->stream);
-                mark(c->ev[2]);
-                launch_dp1_finalize(d, c->score_thld, c->stream);
-                launch_pass_compact(d, c->passidx.as<int>(), c->passdst.as<long long>(), c->passcnt.as<int>(),
-                                    reinterpret_cast<long long*>(c->passcnt.as<char>() + 8), c->stream);
-                mark(c->ev[3]);
-            };
-            if (tc) {
-                phase1(false);
-            } else {
-                CBP_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-                cudaGraph_t g = nullptr;
-                try {
-                    phase1(true);
-                } catch (...) {
-                    cudaStreamEndCapture(c->stream, &g);
-                    if (g) cudaGraphDestroy(g);
-                    throw;
-                }
-                CBP_CUDA(cudaStreamEndCapture(c->stream, &g));
-                if (c->phase1_exec) {
-                    cudaGraphExecUpdateResultInfo info;
-                    if (cudaGraphExecUpdate(c->phase1_exec, g, &info) != cudaSuccess) {
-                        (void)cudaGetLastError();
-                        cudaGraphExecDestroy(c->phase1_exec);
-                        c->phase1_exec = nullptr;
-                    }
-                }
-                if (!c->phase1_exec) {
-                    const cudaError_t e = cudaGraphInstantiate(&c->phase1_exec, g, 0);
-                    if (e != cudaSuccess) {
-                        cudaGraphDestroy(g);
-                        c->phase1_exec = nullptr;
-                        CBP_CUDA(e);
-                    }
-                }
-                cudaGraphDestroy(g);
-                CBP_CUDA(cudaGraphLaunch(c->phase1_exec, c->stream));
-                c->graph_launches += 1;
-            }
-            c->launches += 5;
-            c->stage_launches[0] += 2;
-            c->stage_launches[1] += 1;
-            c->stage_launches[2] += 2;
-            int npass = 0;
-            CBP_CUDA(cudaMemcpyAsync(&npass, c->passcnt.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-            CBP_CUDA(cudaMemcpyAsync(&c->h_dp1err, c->dp1err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-            CBP_CUDA(cudaStreamSynchronize(c->stream));
-            if (c->h_dp1err)
-                throw Error(CBP_ERR_CUDA, "phase-1 DP: a wait for staged score rows timed out");
-            if (tc && c->h_tcerr)
-                throw Error(CBP_ERR_CUDA, "tensor-core contraction: a wait timed out");
-            float ms = 0.f;
-            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
-            c->stage_ms[0] += ms;
-            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]));
-            c->stage_ms[1] += ms;
-            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
-            c->stage_ms[2] += ms;
-            c->last_col0 = s.col0;
-            c->last_ncols = s.ncols;
-            c->last_ld = a.ld;
-            c->last_first_profile = s.p0;
-            c->last_Lq = Lq;
-            c->last_nprof = d.nprof;
-            c->last_npass = npass;
-
-            // statistics and E-values of the passed pairs of this slab
-            if (npass > 0) {
-                c->hitrecs.reserve((size_t)npass * kRecFloats * sizeof(float));
-                StatsArgs st;
-                st.scores = a.scores;
-                st.ld = a.ld;
-                st.Lq = Lq;
-                st.col0 = s.col0;
-                st.p0 = s.p0;
-                st.db = c->db->view;
-                st.qaa = c->query.view.aa;
-                st.qeno = c->query_eno;
-                st.x_uninf = c->opt.x_uninf;
-                st.pass_idx = c->passidx.as<int>();
-                st.pass_dst = c->passdst.as<long long>();
-                st.recs = c->dprecs.as<Dp1Rec>();
-                st.out = c->hitrecs.as<float>();
-                st.nnweights = c->nnweights.as<float>();
-                st.ssemodel = c->opt.ssemodel;
-                st.searchspace = (float)c->searchspace;
-                st.ref_lambda = c->ref_lambda;
-                st.ref_K = c->ref_K;
-                st.exp_gapped_lambda = c->gap_lambda;
-                st.exp_gapped_K = c->gap_K;
-                if (c->opt.tc_form != CBP_TC_PLAIN) {
-                    // the precision forms fit lambda, K, H in FP64 for the E-values
-                    c->fits.reserve((size_t)npass * kFitDoubles * sizeof(double));
-                    st.fits = c->fits.as<double>();
-                    st.use_fit64 = 1;
-                }
-                CBP_CUDA(cudaEventRecord(c->ev[4], c->stream));
-                launch_stats(st, npass, c->stream);
-                CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
-                // the records as the statistics leave them (cbp_read_statistics)
-                c->statrecs.reserve((size_t)npass * kRecFloats * sizeof(float));
-                CBP_CUDA(cudaMemcpyAsync(c->statrecs.p, c->hitrecs.p,
-                                         (size_t)npass * kRecFloats * sizeof(float),
-                                         cudaMemcpyDeviceToDevice, c->stream));
-                c->launches += 1;
-                c->stage_launches[3] += 1;
-
-                // phase-2 MAP realignment of the pairs within the E-value
-                // threshold (in the phase-2 column space of this slab)
-                long long npos2 = 0;
-                CBP_CUDA(cudaMemcpyAsync(&npos2, c->passcnt.as<char>() + 8, sizeof(long long),
-                                         cudaMemcpyDeviceToHost, c->stream));
-                CBP_CUDA(cudaStreamSynchronize(c->stream));
-                const long long nd = map_diag_rows(npos2);
-                const size_t nb = (size_t)map_bands(Lq);
-                const long long alnstride = align_up(npos2 + (long long)npass * Lq, 32);
-                c->alnbuf.reserve(5 * (size_t)alnstride);
-                MapArgs mp;
-                mp.scores = a.scores;
-                mp.modscores = a.modscores;
-                mp.ld = a.ld;
-                mp.Lq = Lq;
-                mp.col0 = s.col0;
-                mp.p0 = s.p0;
-                mp.db = c->db->view;
-                mp.qtrn = c->query.view.trn;
-                mp.qaa = c->query.view.aa;
-                mp.qsss = c->query.view.sss;
-                mp.printsss = c->opt.ssswgt > 0.0f;
-                mp.modscores_inuse = (c->opt.ssswgt > 0.0f || c->opt.cvswgt > 0.0f) ? 1 : 0;
-                mp.minpp = c->opt.minpp;
-                mp.logevthld = c->logE_thld;
-                mp.npass = npass;
-                mp.pass_idx = c->passidx.as<int>();
-                mp.pass_dst = c->passdst.as<long long>();
-                mp.recs = c->hitrecs.as<float>();
-                mp.alns = c->alnbuf.as<char>();
-                mp.alnstride = alnstride;
-                CBP_CUDA(cudaMemsetAsync(c->alnbuf.p, 0, 5 * (size_t)alnstride, c->stream));
-                if (c->opt.mapaln) {
-                    c->cs2.reserve(nb * nd * 32 * sizeof(float));
-                    c->fb2.reserve(nb * nd * 32 * sizeof(float));
-                    c->sg2.reserve(nb * nd * sizeof(unsigned));
-                    c->bt2.reserve(nb * nd * sizeof(unsigned long long));
-                    c->strip2.reserve((size_t)map_strip_floats(npos2) * sizeof(float));
-                    c->maperr.reserve(sizeof(int));
-                    mp.nd = nd;
-                    mp.cs = c->cs2.as<float>();
-                    mp.fb = c->fb2.as<float>();
-                    mp.sg = c->sg2.as<unsigned>();
-                    mp.bt = c->bt2.as<unsigned long long>();
-                    mp.strip = c->strip2.as<float>();
-                    mp.err = c->maperr.as<int>();
-                    CBP_CUDA(cudaMemsetAsync(c->maperr.p, 0, sizeof(int), c->stream));
-                    CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
-                    launch_map(mp, c->stream);
-                    CBP_CUDA(cudaEventRecord(c->ev[7], c->stream));
-                    CBP_CUDA(cudaMemcpyAsync(&c->h_maperr, c->maperr.p, sizeof(int),
-                                             cudaMemcpyDeviceToHost, c->stream));
-                    c->launches += 2;
-                    c->stage_launches[4] += 2;
-                } else {
-                    // MAPALN=0: the phase-1 alignments themselves
-                    // (CuBatchDP::FinalizeALNDynProgDevice)
-                    CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
-                    launch_aln_final(mp, c->btck.as<uint8_t>(), c->dpmax.as<float>(),
-                                     c->dpcoords.as<uint32_t>(), c->stream);
-                    CBP_CUDA(cudaEventRecord(c->ev[7], c->stream));
-                    c->launches += 1;
-                    c->stage_launches[4] += 1;
-                }
-                c->last_npos2 = npos2;
-                // sort keys of this slab's records, for the hit order
-                c->launches += launch_hit_keys(c->hitrecs.as<float>(), npass, c->logE_thld, c->base_npass,
-                                               c->hitkeys.as<uint64_t>(), c->hitcnt.as<int>(), c->stream);
-                c->stage_launches[5] += 1;
-                const size_t off = c->h_recs.size();
-                c->h_recs.resize(off + (size_t)npass * kRecFloats);
-                CBP_CUDA(cudaMemcpyAsync(c->h_recs.data() + off, c->hitrecs.p,
-                                         (size_t)npass * kRecFloats * sizeof(float),
-                                         cudaMemcpyDeviceToHost, c->stream));
-                // this slab's alignment rows go to the running offset of
-                // the whole result (slot of pair K at newDst + K*Lq)
-                const long long shift = c->base_len + c->base_npass * (long long)Lq;
-                const long long slablen = npos2 + (long long)npass * Lq;
-                for (int row = 0; row < 5; row++) {
-                    c->h_alns[row].resize((size_t)(shift + slablen), 0);
-                    CBP_CUDA(cudaMemcpyAsync(c->h_alns[row].data() + shift,
-                                             c->alnbuf.as<char>() + (size_t)row * alnstride,
-                                             (size_t)slablen, cudaMemcpyDeviceToHost, c->stream));
-                }
-                CBP_CUDA(cudaStreamSynchronize(c->stream));
-                if (c->opt.mapaln && c->h_maperr)
-                    throw Error(CBP_ERR_CUDA, "MAP realignment: a wait between the warps of a pair "
-                                              "timed out");
-                CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
-                c->stage_ms[3] += ms;
-                CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]));
-                c->stage_ms[4] += ms;
-                // phase-2 offsets of this slab's pairs become offsets in the
-                // whole result
-                for (size_t i = off; i < c->h_recs.size(); i += kRecFloats) {
-                    uint32_t v;
-                    std::memcpy(&v, &c->h_recs[i + rProNewDst], 4);
-                    v += (uint32_t)c->base_len;
-                    std::memcpy(&c->h_recs[i + rProNewDst], &v, 4);
-                }
-                c->base_len += npos2;
-                c->base_npass += npass;
-            }
-        }
-        // the reported hits in the finalizer's order: one sort over the keys
-        // of all records; the reported ones come first
-        if (c->base_npass > 0) {
-            CBP_CUDA(cudaEventRecord(c->ev[4], c->stream));
-            const int nl = launch_hit_sort(c->hitkeys.as<uint64_t>(), c->base_npass, c->stream);
-            CBP_CUDA(cudaEventRecord(c->ev[5], c->stream));
-            c->launches += nl;
-            c->stage_launches[5] += nl;
-            int nrep = 0;
-            CBP_CUDA(cudaMemcpyAsync(&nrep, c->hitcnt.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-            CBP_CUDA(cudaStreamSynchronize(c->stream));
-            if (nrep < 0 || nrep > c->base_npass) throw Error(CBP_ERR_CUDA, "hit order: inconsistent count");
-            std::vector<uint64_t> keys((size_t)nrep);
-            if (nrep > 0)
-                CBP_CUDA(cudaMemcpyAsync(keys.data(), c->hitkeys.p, (size_t)nrep * sizeof(uint64_t),
-                                         cudaMemcpyDeviceToHost, c->stream));
-            CBP_CUDA(cudaStreamSynchronize(c->stream));
-            c->h_order.resize((size_t)nrep);
-            for (int i = 0; i < nrep; i++) c->h_order[i] = (int32_t)(uint32_t)keys[i];
-            float ms = 0.f;
-            CBP_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
-            c->stage_ms[5] += ms;
-        }
-        CBP_CUDA(cudaStreamSynchronize(c->stream));
+        if (nqueries) *nqueries = c->res.size();
+        if (k >= c->res.size()) throw Error(CBP_ERR_ARG, "query index beyond the last call's queries");
+        c->cur = k;
     });
 }
 
@@ -1223,12 +1380,13 @@ int cbp_read_score_matrix(cbp_context* c, float* scores, float* modscores, size_
         if (ncols) *ncols = (size_t)c->last_ncols;
         if (first_profile) *first_profile = (size_t)c->last_first_profile;
         const size_t w = (size_t)c->last_ncols * sizeof(float);
+        const size_t r0 = (size_t)(c->last_row0 * c->last_ld);
         if (scores)
-            CBP_CUDA(cudaMemcpy2D(scores, ld * sizeof(float), c->scores.p, c->last_ld * sizeof(float), w,
-                                  c->last_Lq, cudaMemcpyDeviceToHost));
-        if (modscores)
-            CBP_CUDA(cudaMemcpy2D(modscores, ld * sizeof(float), c->modscores.p, c->last_ld * sizeof(float),
+            CBP_CUDA(cudaMemcpy2D(scores, ld * sizeof(float), c->scores.as<float>() + r0, c->last_ld * sizeof(float),
                                   w, c->last_Lq, cudaMemcpyDeviceToHost));
+        if (modscores)
+            CBP_CUDA(cudaMemcpy2D(modscores, ld * sizeof(float), c->modscores.as<float>() + r0,
+                                  c->last_ld * sizeof(float), w, c->last_Lq, cudaMemcpyDeviceToHost));
     });
 }
 
@@ -1243,7 +1401,8 @@ int cbp_read_phase1(cbp_context* c, float* score, float* psts, uint32_t* beg, ui
         if (npass) *npass = (size_t)c->last_npass;
         if (nmax < n) throw Error(CBP_ERR_ARG, "output arrays too small");
         std::vector<Dp1Rec> r(n);
-        CBP_CUDA(cudaMemcpy(r.data(), c->dprecs.p, n * sizeof(Dp1Rec), cudaMemcpyDeviceToHost));
+        CBP_CUDA(cudaMemcpy(r.data(), c->dprecs.as<Dp1Rec>() + c->last_dp_off, n * sizeof(Dp1Rec),
+                            cudaMemcpyDeviceToHost));
         for (size_t i = 0; i < n; i++) {
             if (score) score[i] = r[i].score;
             if (psts) psts[i] = r[i].psts;
@@ -1252,8 +1411,8 @@ int cbp_read_phase1(cbp_context* c, float* score, float* psts, uint32_t* beg, ui
             if (passed) passed[i] = r[i].passed;
         }
         if (pass_list && c->last_npass > 0)
-            CBP_CUDA(cudaMemcpy(pass_list, c->passidx.p, (size_t)c->last_npass * sizeof(int),
-                                cudaMemcpyDeviceToHost));
+            CBP_CUDA(cudaMemcpy(pass_list, c->passidx.as<int>() + c->last_dp_off,
+                                (size_t)c->last_npass * sizeof(int), cudaMemcpyDeviceToHost));
     });
 }
 
@@ -1293,7 +1452,8 @@ int cbp_read_btck(cbp_context* c, uint8_t* btck, size_t ld)
         check_ctx(c);
         if (!c->last_Lq) throw Error(CBP_ERR_STATE, "no processed query");
         if (ld < (size_t)c->last_ncols) throw Error(CBP_ERR_ARG, "ld smaller than the slab width");
-        CBP_CUDA(cudaMemcpy2D(btck, ld, c->btck.p, c->last_ld, (size_t)c->last_ncols, c->last_Lq,
+        CBP_CUDA(cudaMemcpy2D(btck, ld, c->btck.as<uint8_t>() + c->last_row0 * c->last_ld, c->last_ld,
+                              (size_t)c->last_ncols, c->last_Lq,
                               cudaMemcpyDeviceToHost));
     });
 }
@@ -1310,14 +1470,15 @@ int cbp_read_slab_columns(cbp_context* c, size_t first_col, size_t ncols, float*
         if (ncols == 0) return;
         CBP_CUDA(cudaStreamSynchronize(c->stream));
         const size_t w = ncols * sizeof(float);
+        const size_t r0 = (size_t)(c->last_row0 * c->last_ld);
         if (scores)
-            CBP_CUDA(cudaMemcpy2D(scores, ld * sizeof(float), (const float*)c->scores.p + first_col,
+            CBP_CUDA(cudaMemcpy2D(scores, ld * sizeof(float), (const float*)c->scores.p + r0 + first_col,
                                   c->last_ld * sizeof(float), w, c->last_Lq, cudaMemcpyDeviceToHost));
         if (modscores)
-            CBP_CUDA(cudaMemcpy2D(modscores, ld * sizeof(float), (const float*)c->modscores.p + first_col,
+            CBP_CUDA(cudaMemcpy2D(modscores, ld * sizeof(float), (const float*)c->modscores.p + r0 + first_col,
                                   c->last_ld * sizeof(float), w, c->last_Lq, cudaMemcpyDeviceToHost));
         if (btck)
-            CBP_CUDA(cudaMemcpy2D(btck, ld, (const uint8_t*)c->btck.p + first_col, c->last_ld, ncols,
+            CBP_CUDA(cudaMemcpy2D(btck, ld, (const uint8_t*)c->btck.p + r0 + first_col, c->last_ld, ncols,
                                   c->last_Lq, cudaMemcpyDeviceToHost));
     });
 }
@@ -1326,11 +1487,12 @@ int cbp_get_hit_records(cbp_context* c, float* recs, size_t max_records, size_t*
 {
     return guarded([&] {
         check_ctx(c);
-        const size_t n = c->h_recs.size() / kRecFloats;
+        const QueryResult& r = cur_result(c);
+        const size_t n = r.h_recs.size() / kRecFloats;
         if (nrecords) *nrecords = n;
         if (recs) {
             if (max_records < n) throw Error(CBP_ERR_ARG, "record buffer too small");
-            std::memcpy(recs, c->h_recs.data(), c->h_recs.size() * sizeof(float));
+            std::memcpy(recs, r.h_recs.data(), r.h_recs.size() * sizeof(float));
         }
     });
 }
@@ -1341,9 +1503,10 @@ int cbp_get_hit_list(cbp_context* c, int32_t* order, size_t max_hits, size_t* nh
         check_ctx(c);
         // ordered on the device at the end of cbp_process; the first
         // max_hits entries are the top max_hits hits
-        const size_t n = c->h_order.size();
+        const QueryResult& r = cur_result(c);
+        const size_t n = r.h_order.size();
         if (nhits) *nhits = n;
-        if (order && n) std::memcpy(order, c->h_order.data(), std::min(n, max_hits) * sizeof(int32_t));
+        if (order && n) std::memcpy(order, r.h_order.data(), std::min(n, max_hits) * sizeof(int32_t));
     });
 }
 
@@ -1351,11 +1514,12 @@ int cbp_get_alignments(cbp_context* c, char* rows, size_t row_stride, size_t* le
 {
     return guarded([&] {
         check_ctx(c);
-        const size_t n = c->h_alns[0].size();
+        const QueryResult& q = cur_result(c);
+        const size_t n = q.h_alns[0].size();
         if (length) *length = n;
         if (rows) {
             if (row_stride < n) throw Error(CBP_ERR_ARG, "row stride smaller than the alignment rows");
-            for (int r = 0; r < 5; r++) std::memcpy(rows + (size_t)r * row_stride, c->h_alns[r].data(), n);
+            for (int r = 0; r < 5; r++) std::memcpy(rows + (size_t)r * row_stride, q.h_alns[r].data(), n);
         }
     });
 }
@@ -1368,16 +1532,17 @@ int cbp_format_hits(cbp_context* c, const cbp_format_options* fo, const char* co
         check_ctx(c);
         if (!c->have_db) throw Error(CBP_ERR_STATE, "no database chunk transferred");
         const ProfilesStore& db = *c->db;
-        const size_t n = c->h_alns[0].size();
+        const QueryResult& q = cur_result(c);
+        const size_t n = q.h_alns[0].size();
         std::vector<char> rows(5 * n);
         for (int r = 0; r < 5; r++)
-            if (n) std::memcpy(rows.data() + (size_t)r * n, c->h_alns[r].data(), n);
-        const int qss = c->query.h_ss.empty() ? 1 : c->query.h_ss[0];
-        rc = format_hits_from(c->h_recs.data(), c->h_recs.size() / kRecFloats, c->h_order.data(),
-                              c->h_order.size(), rows.data(), n, n,
+            if (n) std::memcpy(rows.data() + (size_t)r * n, q.h_alns[r].data(), n);
+        const int qss = c->query.h_ss.empty() ? 1 : c->query.h_ss[c->cur];
+        rc = format_hits_from(q.h_recs.data(), q.h_recs.size() / kRecFloats, q.h_order.data(),
+                              q.h_order.size(), rows.data(), n, n,
                               db.h_plen.data(), db.h_eno.data(), db.h_ss.empty() ? nullptr : db.h_ss.data(),
-                              db.h_plen.size(), descs, c->last_Lq, c->query_eno, qss, c->opt.ssswgt,
-                              c->logE_thld, (float)c->searchspace, fo, buf, cap, used, nhits);
+                              db.h_plen.size(), descs, q.Lq, q.eno, qss, c->opt.ssswgt,
+                              q.logE_thld, (float)q.searchspace, fo, buf, cap, used, nhits);
     });
     return grc != CBP_OK ? grc : rc;
 }
@@ -1386,8 +1551,9 @@ int cbp_get_search_space(cbp_context* c, uint64_t* search_space, size_t* delta_l
 {
     return guarded([&] {
         check_ctx(c);
-        if (search_space) *search_space = c->searchspace;
-        if (delta_length) *delta_length = c->delta_length;
+        const QueryResult& r = cur_result(c);
+        if (search_space) *search_space = r.searchspace;
+        if (delta_length) *delta_length = r.delta_length;
     });
 }
 

@@ -375,11 +375,20 @@ score_matrix_kernel(const ScoreArgs a)
         float acc = 0.0f;
         if (a.dots_in_scores) {
             acc = a.scores[(long long)row * a.ld + col];
-        } else {
+        } else if (a.q.P == 1) {
 #pragma unroll
             for (int k = 0; k < kNAA; k++) {
                 const float num = s_qtf[r][k] * s_dtf[k][lane];
                 const float den = 0.5f * (s_qbg[k] + s_dbg[k][lane]);
+                acc = acc + __fdiv_rn(num, den);
+            }
+        } else {
+            // stacked queries: the background of this row's query
+            const float* __restrict__ qbg = a.q.bkg + a.q.pro[row];
+#pragma unroll
+            for (int k = 0; k < kNAA; k++) {
+                const float num = s_qtf[r][k] * s_dtf[k][lane];
+                const float den = 0.5f * (__ldg(qbg + (long long)k * a.q.P) + s_dbg[k][lane]);
                 acc = acc + __fdiv_rn(num, den);
             }
         }

@@ -200,7 +200,7 @@ tc_query_image_kernel(const TcArgs a, uint8_t* __restrict__ img, int ntiles)
     uint32_t hi[20], lo[20];
 #pragma unroll
     for (int k = 0; k < 20; k++) {
-        const float x = r < a.Lq ? a.q.tf[(long long)k * a.q.N + r] : 0.0f;
+        const float x = r < a.Lq ? a.q.tf[(long long)k * a.q.N + a.qrow0 + r] : 0.0f;
         split<kBf16>(x, hi[k], lo[k]);
     }
     const int t = r / kTNMax, rr = r - t * kTNMax;
@@ -250,7 +250,8 @@ tc_umma_kernel(const TcArgs a, const uint8_t* __restrict__ qimg, float* __restri
                 const int p = a.db.pro[g];
 #pragma unroll
                 for (int k = 0; k < 20; k++) {
-                    const float den = 0.5f * (a.q.bkg[k] + a.db.bkg[(long long)k * a.db.P + p]);
+                    const float den = 0.5f * (a.q.bkg[(long long)k * a.q.P + a.qprof] +
+                                              a.db.bkg[(long long)k * a.db.P + p]);
                     split<kBf16>(__fdiv_rn(a.db.tf[(long long)k * a.db.N + g], den), hi[k], lo[k]);
                 }
             } else {

@@ -13,7 +13,9 @@ struct TcArgs {
     long long col0 = 0;   // first chunk position of the slab
     int ncols = 0;        // slab positions
     long long ld = 0;     // leading dimension of the score matrix
-    int Lq = 0;
+    int Lq = 0;           // rows of this query
+    int qrow0 = 0;        // its first position in the (stacked) query profile set
+    int qprof = 0;        // its profile index there (for its background)
 };
 
 // bytes of the query operand image for a query of Lq positions

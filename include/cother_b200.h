@@ -211,6 +211,27 @@ int cbp_slab_bytes(const cbp_options* opt, size_t query_len, size_t positions, s
 int cbp_process(cbp_context* ctx, int query_serial, size_t query_len,
                 char* const* qpmbeg, char* const* qpmend);
 
+/* Search several queries against the resident chunk in one pass over its
+ * database columns: the queries' rows are stacked into one score matrix per
+ * slab (one column-order and one score-kernel launch for all of them), and
+ * each query's phase 1 follows in the same CUDA graph; statistics, MAP and
+ * the hit order then run per query. Each query's results are what
+ * cbp_process would give for it alone (thresholds from EVAL for its own
+ * length unless set; cbp_set_query_len applies to single queries only).
+ * The result calls (cbp_get_hit_records, cbp_get_alignments,
+ * cbp_get_hit_list, cbp_format_hits, cbp_get_search_space) read query 0
+ * after the call; cbp_select_query chooses another. The inspection calls
+ * (cbp_read_*) see the last query. No counterpart in the reference, which
+ * searches one query per ProcessScoreMatrix call
+ * (src/libmycu/cualn/DevCommThread.cpp:316-355). */
+int cbp_process_batch(cbp_context* ctx, size_t nqueries, const size_t* query_lens,
+                      char* const* const* qpmbeg, char* const* const* qpmend);
+
+/* Make query k of the last cbp_process/cbp_process_batch call the one the
+ * result calls read; *nqueries (may be NULL) receives the call's number of
+ * queries. CBP_ERR_ARG when k is out of range. */
+int cbp_select_query(cbp_context* ctx, size_t k, size_t* nqueries);
+
 /* Wait until no work of this context is in flight (WaitForIdleChilds). */
 int cbp_wait_idle(cbp_context* ctx);
 
