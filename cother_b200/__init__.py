@@ -80,6 +80,16 @@ def load_library(path: str | None = None):
         "cbp_transfer_chunk": (i32, [vp, vp, vp, vp]),
         "cbp_process": (i32, [vp, i32, sz, vp, vp]),
         "cbp_process_batch": (i32, [vp, sz, vp, vp, vp]),
+        "cbp_ledger_choose": (i32, [vp, vp, sz, sz, sz, sz, ctypes.POINTER(sz)]),
+        "cbp_server_default_config": (None, [vp]),
+        "cbp_server_create": (i32, [vp, vp, vp, vp, vp, ctypes.POINTER(vp)]),
+        "cbp_server_budget": (i32, [vp, ctypes.POINTER(sz)]),
+        "cbp_server_submit": (i32, [vp, sz, vp, vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "cbp_server_wait": (i32, [vp, ctypes.c_uint64, i32, vp]),
+        "cbp_server_get": (i32, [vp, ctypes.c_uint64, vp, sz, vp, sz, vp, sz]),
+        "cbp_server_release": (i32, [vp, ctypes.c_uint64]),
+        "cbp_server_destroy": (i32, [vp]),
+        "cbp_server_last_error": (ctypes.c_char_p, []),
         "cbp_select_query": (i32, [vp, sz, ctypes.POINTER(sz)]),
         "cbp_wait_idle": (i32, [vp]),
         "cbp_read_score_matrix": (i32, [vp, vp, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
@@ -165,6 +175,27 @@ def slab_bytes(query_len: int, positions: int, options: "Options | None" = None)
     _check(load_library().cbp_slab_bytes(ctypes.byref(o), int(query_len), int(positions),
                                          ctypes.byref(n)))
     return int(n.value)
+
+
+def alignments_from(recs: np.ndarray, rows: np.ndarray, query_len: int, db_lens) -> list:
+    """Per record: its alignment rows (query, middle, target, query SS,
+    target SS) as strings, or None when it was not realigned. `rows` are the
+    5 alignment rows of a search; the pair of record k ends its slot at
+    newDst + Ld - 1 + (k+1) Lq (the finalizer's layout,
+    src/libmycu/cupro/CuBatchProcessingFinalizerPlain.cpp:252-256)."""
+    t = records_table(recs)
+    out = []
+    alnlen = t["log_evalue_pair"].view(np.int32)
+    for k in range(len(t["score"])):
+        n = int(alnlen[k])
+        if n <= 0:
+            out.append(None)
+            continue
+        p = int(t["org_pro_no"][k])
+        Ld = int(db_lens[p])
+        term = int(t["pro_new_dst"][k]) + k * query_len + Ld + query_len - 1
+        out.append(tuple(bytes(rows[r, term - n:term]).decode() for r in range(5)))
+    return out
 
 
 def records_table(recs: np.ndarray) -> dict:
@@ -378,20 +409,7 @@ class BatchProcessing:
     def alignments(self, query_len: int):
         """Per hit: (query, middle, target, query SS, target SS) strings, or
         None for hits that were not realigned."""
-        recs = records_table(self.hit_records())
-        rows = self.alignment_rows()
-        out = []
-        alnlen = recs["log_evalue_pair"].view(np.int32)
-        for k in range(len(recs["score"])):
-            n = int(alnlen[k])
-            if n <= 0:
-                out.append(None)
-                continue
-            p = int(recs["org_pro_no"][k])
-            Ld = int(self._db.lens[p])
-            term = int(recs["pro_new_dst"][k]) + k * query_len + Ld + query_len - 1
-            out.append(tuple(bytes(rows[r, term - n:term]).decode() for r in range(5)))
-        return out
+        return alignments_from(self.hit_records(), self.alignment_rows(), query_len, self._db.lens)
 
     def hit_list(self, top: int | None = None) -> np.ndarray:
         """Record indices of the reported hits of the last search (log E at

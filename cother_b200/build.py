@@ -36,6 +36,7 @@ CUDA_SOURCES = [
     "tc_kernel.cu",
     "hits_kernel.cu",
     "format.cpp",
+    "server.cpp",
     "dbfile.cpp",
 ]
 CUDA_HEADERS = [

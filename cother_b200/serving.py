@@ -1,32 +1,35 @@
-"""A request loop over a resident database.
+"""A request loop over a resident database (the C++ server of the library).
 
-Several search contexts (slots) share one device copy of the database
-(``BatchProcessing.share_database``); each has its own CUDA stream, working
-memory and host thread, so the searches of the requests in flight overlap on
-the device. Requests are admitted in arrival order as a slot and enough
-working memory free up: a request's footprint is what its score matrices,
-DP buffers and alignment rows take for one slab of the database (the slab
-planner's charge, ``cother_b200.slab_bytes``), with the slab cut so that a
-request never needs more than ``max_share`` of the budget. A slot keeps its buffers between requests (they
-only grow), so the ledger charges each slot the largest footprint it has
-held, and admits a request only if the sum over slots stays within the
-budget.
+The server (``cbp_server_*`` in ``include/cother_b200.h``, host C++ in
+``csrc/server.cpp``) keeps one database chunk resident on a GPU and searches
+queries as they arrive: `slots` search contexts share the chunk, each with
+its own stream, working memory and worker thread, so that the batches in
+flight overlap on the device. When a slot is free, the oldest waiting query
+and the ones behind it (up to `max_batch`) are searched together in one pass
+over the database -- their rows stacked into one score matrix per slab.
+Batches are admitted in arrival order by their memory footprint: a batch is
+charged what one slab of its stacked rows takes (``cother_b200.slab_bytes``),
+the slab cut so that one batch takes at most `max_share` of the budget, and a
+slot is charged the largest footprint it has held (its buffers only grow);
+a batch starts only while the sum over the slots stays within the budget.
+
+This module binds that server with ctypes: :class:`SearchServer` returns a
+Future per query, resolved with its hits, records and times.
 
 The reference has no request loop (it is a batch program); this is the
 serving form of the same search path.
 """
 from __future__ import annotations
 
-import collections
-import threading
-import time
-from concurrent.futures import Future
-from dataclasses import dataclass, field
+import ctypes
+from concurrent.futures import Future, ThreadPoolExecutor
 
 import numpy as np
 
+
 def slab_cost(query_len: int, options=None):
-    """(bytes per slab position, bytes per slab) charged for a query."""
+    """(bytes per slab position, bytes per slab) charged for `query_len`
+    stacked query rows."""
     import cother_b200 as cb
     fixed = cb.slab_bytes(query_len, 0, options)
     return cb.slab_bytes(query_len, 1, options) - fixed, fixed
@@ -37,139 +40,92 @@ def footprint(query_len: int, slab_positions: int, options=None) -> int:
     return fixed + per_pos * int(slab_positions)
 
 
-def slab_positions_for(query_len: int, db_positions: int, budget: int, max_share: float,
-                       options=None) -> int:
-    """Largest slab (positions) whose footprint fits max_share of the budget."""
-    per_pos, fixed = slab_cost(query_len, options)
-    cap = max(0, int(budget * max_share) - fixed) // per_pos
-    return max(1, min(int(db_positions), cap))
+def ledger_choose(held, busy, budget: int, need: int, min_grant: int = 1):
+    """The server's admission rule (cbp_ledger_choose): (slot, granted
+    bytes) for a batch of footprint `need` given each slot's charge `held`
+    and `busy` flags, or (None, 0) to wait."""
+    import cother_b200 as cb
+    L = cb.load_library()
+    n = len(held)
+    h = (ctypes.c_size_t * n)(*[int(x) for x in held])
+    b = (ctypes.c_char * n)(*[bytes([1 if x else 0]) for x in busy])
+    g = ctypes.c_size_t()
+    i = L.cbp_ledger_choose(h, b, n, int(budget), int(need), int(min_grant), ctypes.byref(g))
+    return (None, 0) if i < 0 else (i, g.value)
 
 
-@dataclass
-class Request:
-    query: object
-    arrival: float
-    future: Future = field(default_factory=Future)
-    slab: int = 0
-    need: int = 0
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("budget_bytes", ctypes.c_size_t), ("max_share", ctypes.c_double),
+                ("db_len", ctypes.c_uint64), ("n_seqs", ctypes.c_size_t)]
 
 
-class Ledger:
-    """Admission by memory footprint (pure host logic).
+class ServerResult(ctypes.Structure):
+    _fields_ = [("arrival_s", ctypes.c_double), ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double),
+                ("slot", ctypes.c_int), ("batch", ctypes.c_int), ("slab_positions", ctypes.c_size_t),
+                ("nrecords", ctypes.c_size_t), ("nhits", ctypes.c_size_t),
+                ("alignment_length", ctypes.c_size_t)]
 
-    A slot's buffers only grow, so each slot is charged the largest
-    footprint it has held. A request gets its full footprint on a free slot
-    when the charge stays within the budget; if it does not fit now but
-    would fit on a busy slot once that finishes, it waits; otherwise (no
-    slot will ever have room for all of it) it gets what the roomiest free
-    slot can hold, at least `min_grant`, and runs with a smaller slab."""
 
-    def __init__(self, nslots: int, budget: int):
-        self.held = [0] * nslots
-        self.busy = [False] * nslots
-        self.budget = int(budget)
-
-    def choose(self, need: int, min_grant: int = 1):
-        """(slot, granted bytes) for a request of footprint `need`, or
-        (None, 0) to wait."""
-        total = sum(self.held)
-        best, best_growth = None, None
-        for i, b in enumerate(self.busy):
-            if b:
-                continue
-            growth = max(0, need - self.held[i])
-            if total + growth <= self.budget and (best is None or growth < best_growth):
-                best, best_growth = i, growth
-        if best is not None:
-            return best, need
-        if any(b and total + max(0, need - self.held[i]) <= self.budget
-               for i, b in enumerate(self.busy)):
-            return None, 0
-        room = [(self.budget - (total - self.held[i]), i) for i, b in enumerate(self.busy) if not b]
-        if not room:
-            return None, 0
-        avail, i = max(room)
-        return (i, avail) if avail >= min_grant else (None, 0)
-
-    def take(self, i: int, grant: int) -> None:
-        self.busy[i] = True
-        self.held[i] = max(self.held[i], grant)
-        assert sum(self.held) <= self.budget
-
-    def give_back(self, i: int) -> None:
-        self.busy[i] = False
+class ServerError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
 
 
 class SearchServer:
     """Serve search requests against one resident database.
 
-    `run_search(slot, request)` does the search of one request on one slot;
-    the default runs the CUDA path through the slot's BatchProcessing
-    context. Results are delivered through the Future returned by submit():
-    a dict with the hit list (``cother_b200.sharding.Hit``), the records,
-    and the request's arrival, start and finish times."""
+    submit(query) returns a Future resolved with a dict: the hit list
+    (``cother_b200.sharding.Hit``, in the finalizer's order), the records,
+    the request's arrival, start and finish times (seconds of a steady
+    clock), its slot, the size of its batch and the slab it ran with."""
 
-    def __init__(self, db, ss_table, options=None, slots: int = 3, budget: int | None = None,
-                 max_share: float = 0.5, device: int = 0, db_len: int | None = None,
-                 n_seqs: int | None = None, run_search=None):
+    def __init__(self, db, ss_table, options=None, slots: int = 3, max_batch: int = 4,
+                 budget: int | None = None, max_share: float = 0.5, device: int = 0,
+                 db_len: int | None = None, n_seqs: int | None = None):
+        import cother_b200 as cb
+        L = cb.load_library()
+        self._L = L
         self.db = db
-        self.options = options
-        self._longest = int(np.max(db.lens))   # a slab holds whole profiles
-        self.nslots = int(slots)
-        self.max_share = float(max_share)
-        self._cv = threading.Condition()
-        self._queue = collections.deque()
-        self._stop = False
-        self._done = False
-        self._contexts = []
-        self._run = run_search or self._run_cuda
-        if run_search is None:
-            import cother_b200 as cb
-            owner = cb.BatchProcessing(ss_table, options, device=device, dev_mem_bytes=1 << 20)
-            owner.transfer_cpm_data(db)
-            if budget is None:
-                # what is free once the database is resident
-                budget = int(cb.device_memory(device)[0] * 0.7)
-            for _ in range(self.nslots):
-                bp = cb.BatchProcessing(ss_table, options, device=device, dev_mem_bytes=budget)
-                bp.share_database(owner)
-                bp.set_db_details(db_len or db.npositions, n_seqs or db.nprofiles)
-                self._contexts.append(bp)
-            self._owner = owner
-        self.ledger = Ledger(self.nslots, budget if budget is not None else 1 << 62)
-        self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True)
-                         for i in range(self.nslots)]
-        self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
-        self._assigned = [None] * self.nslots
-        for t in self._threads:
-            t.start()
-        self._dispatcher.start()
+        self.options = options or cb.Options.defaults()
+        cfg = ServerConfig()
+        L.cbp_server_default_config(ctypes.byref(cfg))
+        cfg.device = int(device)
+        cfg.slots = int(slots)
+        cfg.max_batch = int(max_batch)
+        cfg.budget_bytes = int(budget or 0)
+        cfg.max_share = float(max_share)
+        cfg.db_len = int(db_len or 0)
+        cfg.n_seqs = int(n_seqs or 0)
+        self._ss = np.ascontiguousarray(ss_table, np.float32)
+        beg, end = db.field_tables()
+        h = ctypes.c_void_p()
+        self._check(L.cbp_server_create(ctypes.byref(cfg), ctypes.byref(self.options), self._ss.ctypes.data,
+                                        beg, end, ctypes.byref(h)))
+        self._h = h
+        b = ctypes.c_size_t()
+        self._check(L.cbp_server_budget(self._h, ctypes.byref(b)))
+        self.budget = b.value
+        self._pool = ThreadPoolExecutor(max_workers=256)
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            msg = self._L.cbp_server_last_error()
+            raise ServerError(rc, msg.decode() if msg else "")
 
     # -- public -------------------------------------------------------------
     def submit(self, query) -> Future:
-        r = Request(query=query, arrival=time.perf_counter())
-        r.slab = slab_positions_for(query.npositions, self.db.npositions, self.ledger.budget,
-                                    self.max_share, self.options)
-        if r.slab < min(self._longest, self.db.npositions):
-            raise ValueError("the memory budget cannot hold one slab of the longest profile "
-                             "for this query length")
-        r.need = footprint(query.npositions, r.slab, self.options)
-        with self._cv:
-            self._queue.append(r)
-            self._cv.notify_all()
-        return r.future
+        beg, end = query.field_tables()
+        t = ctypes.c_uint64()
+        self._check(self._L.cbp_server_submit(self._h, int(query.npositions), beg, end, ctypes.byref(t)))
+        return self._pool.submit(self._collect, t.value, int(query.npositions))
 
     def close(self) -> None:
-        with self._cv:
-            self._stop = True
-            self._cv.notify_all()
-        self._dispatcher.join()
-        for t in self._threads:
-            t.join()
-        for bp in self._contexts:
-            bp.close()
-        if self._contexts:
-            self._owner.close()
+        if getattr(self, "_h", None):
+            self._L.cbp_server_destroy(self._h)     # finishes the queued requests
+            self._h = None
+            self._pool.shutdown(wait=True)
 
     def __enter__(self):
         return self
@@ -178,55 +134,25 @@ class SearchServer:
         self.close()
 
     # -- internals ------------------------------------------------------------
-    def _dispatch(self) -> None:
-        with self._cv:
-            while True:
-                while not self._stop and not self._queue:
-                    self._cv.wait()
-                if not self._queue:            # stopped and drained
-                    self._done = True
-                    self._cv.notify_all()
-                    return
-                head = self._queue[0]          # first come, first served
-                per_pos, fixed = slab_cost(head.query.npositions, self.options)
-                i, grant = self.ledger.choose(head.need, fixed + per_pos * self._longest)
-                if i is None:
-                    self._cv.wait()
-                    continue
-                self._queue.popleft()
-                if grant < head.need:
-                    head.slab = (grant - fixed) // per_pos
-                    head.need = footprint(head.query.npositions, head.slab, self.options)
-                self.ledger.take(i, head.need)
-                self._assigned[i] = head
-                self._cv.notify_all()
-
-    def _worker(self, i: int) -> None:
-        while True:
-            with self._cv:
-                while self._assigned[i] is None and not self._done:
-                    self._cv.wait()
-                r = self._assigned[i]
-                if r is None:
-                    return
-            start = time.perf_counter()
-            try:
-                result = self._run(i, r)
-                result.update(arrival=r.arrival, start=start, finish=time.perf_counter(), slot=i)
-                r.future.set_result(result)
-            except Exception as e:  # noqa: BLE001 - handed to the caller
-                r.future.set_exception(e)
-            with self._cv:
-                self._assigned[i] = None
-                self.ledger.give_back(i)
-                self._cv.notify_all()
-
-    def _run_cuda(self, i: int, r: Request) -> dict:
-        from cother_b200.sharding import local_hits
-        bp = self._contexts[i]
-        bp.set_max_slab_positions(r.slab)
-        bp.process_score_matrix(r.query)
-        return {"hits": local_hits(bp, 0, r.query.npositions), "records": bp.hit_records()}
+    def _collect(self, ticket: int, query_len: int) -> dict:
+        import cother_b200 as cb
+        from .sharding import Hit
+        L = self._L
+        info = ServerResult()
+        self._check(L.cbp_server_wait(self._h, ticket, -1, ctypes.byref(info)))
+        recs = np.zeros((info.nrecords, cb.REC_FLOATS), np.float32)
+        order = np.zeros(info.nhits, np.int32)
+        n = int(info.alignment_length)
+        rows = np.zeros((5, max(n, 1)), np.uint8)
+        self._check(L.cbp_server_get(self._h, ticket, recs.ctypes.data, info.nrecords, order.ctypes.data,
+                                     info.nhits, rows.ctypes.data, rows.shape[1]))
+        L.cbp_server_release(self._h, ticket)
+        alns = cb.alignments_from(recs, rows[:, :n], query_len, self.db.lens)
+        tab = cb.records_table(recs)
+        hits = [Hit(profile=int(tab["org_pro_no"][i]), log_evalue=float(recs[i, 8]), record=recs[i].copy(),
+                    alignment=alns[i]) for i in order]
+        return {"hits": hits, "records": recs, "arrival": info.arrival_s, "start": info.start_s,
+                "finish": info.finish_s, "slot": info.slot, "batch": info.batch, "slab": info.slab_positions}
 
 
 def latency_summary(results) -> dict:
@@ -237,4 +163,5 @@ def latency_summary(results) -> dict:
     t1 = max(x["finish"] for x in results)
     return {"queries": len(results), "queries_per_s": len(results) / (t1 - t0),
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "service_p50_ms": float(np.percentile(svc, 50))}
+            "service_p50_ms": float(np.percentile(svc, 50)),
+            "mean_batch": float(np.mean([x.get("batch", 1) for x in results]))}

@@ -492,6 +492,81 @@ int cbp_dp1_noalloc(const float* scores, size_t ld, int query_len, const float* 
                     uint8_t* btck, float* max_scores, uint32_t* max_coords,
                     void* stream);
 
+/* ------------------------------------------------------------------------
+ * Request loop over a resident database (serving). No counterpart in the
+ * reference, which is a batch program: its job dispatcher hands whole
+ * queries to per-GPU workers (src/libmycu/cualn/JobDispatcher.cpp:1124-1133),
+ * each searching one query at a time (DevCommThread.cpp:316-355).
+ *
+ * A server keeps one database chunk resident on a GPU and searches queries
+ * as they arrive, through `slots` contexts sharing the chunk (each with its
+ * own stream, working memory and worker thread). When a slot is free the
+ * oldest waiting query and the ones behind it, up to `max_batch`, are
+ * searched together in one pass over the database (cbp_process_batch), as
+ * long as the stacked queries' slab still holds the longest profile. A
+ * batch is charged the device memory of one slab of its stacked rows
+ * (cbp_slab_bytes), the slab cut so that a batch takes at most `max_share`
+ * of the budget; batches are admitted in arrival order while the charges
+ * of all slots (each slot's largest so far) stay within the budget. */
+typedef struct cbp_server cbp_server;
+
+typedef struct cbp_server_config {
+    int device;             /* GPU */
+    int slots;              /* concurrent batches (contexts), 1..64 */
+    int max_batch;          /* queries searched in one pass at most */
+    size_t budget_bytes;    /* device memory for the slots' working buffers
+                             * (0 = 70 % of the free memory after the upload) */
+    double max_share;       /* largest share of the budget one batch may take */
+    uint64_t db_len;        /* database totals for E-values (0 = the chunk's) */
+    size_t n_seqs;
+} cbp_server_config;
+
+/* Times (seconds of a steady clock) and shape of a finished request. */
+typedef struct cbp_server_result {
+    double arrival_s, start_s, finish_s;
+    int slot, batch;                 /* the slot that searched it, queries in its batch */
+    size_t slab_positions;           /* slab size the batch was searched with */
+    size_t nrecords, nhits, alignment_length;
+} cbp_server_result;
+
+/* The admission rule (host only, no device): for a batch needing `need`
+ * bytes, the free slot (busy[i] == 0) whose growth of its charge held[i]
+ * keeps the sum within `budget`, the least growth first, with
+ * *grant = need; -1 (wait) while a busy slot would have room once done;
+ * else the free slot with the most room, if that is at least min_grant,
+ * with *grant = its room (the batch then runs with a smaller slab). */
+int cbp_ledger_choose(const size_t* held, const char* busy, size_t nslots, size_t budget, size_t need,
+                      size_t min_grant, size_t* grant);
+
+/* slots 3, max_batch 4, budget 0 (auto), max_share 0.5, totals 0 */
+void cbp_server_default_config(cbp_server_config* cfg);
+/* Upload the chunk (the 181 field pointer tables, as cbp_transfer_chunk
+ * takes them) and start the server's threads. */
+int cbp_server_create(const cbp_server_config* cfg, const cbp_options* opt, const float* ss_table,
+                      char* const* db_pmbeg, char* const* db_pmend, cbp_server** server);
+/* The memory budget the server admits batches against. */
+int cbp_server_budget(cbp_server* server, size_t* budget_bytes);
+/* Queue a query (its field tables are copied; the caller may free them on
+ * return); *ticket identifies the request. CBP_ERR_MEMORY when the budget
+ * cannot hold a slab of the longest profile for this query. */
+int cbp_server_submit(cbp_server* server, size_t query_len, char* const* qpmbeg, char* const* qpmend,
+                      uint64_t* ticket);
+/* Wait for a request (timeout_ms < 0: without limit; CBP_ERR_STATE when it
+ * is not done in time); *info (may be NULL) receives its times and sizes.
+ * Returns the search's status. */
+int cbp_server_wait(cbp_server* server, uint64_t ticket, int timeout_ms, cbp_server_result* info);
+/* A finished request's results: hit records (CBP_REC_FLOATS each), the
+ * first max_hits of its hit order, the 5 alignment rows (row_stride >= the
+ * alignment length). Any output may be NULL. */
+int cbp_server_get(cbp_server* server, uint64_t ticket, float* records, size_t max_records,
+                   int32_t* order, size_t max_hits, char* rows, size_t row_stride);
+/* Forget a finished request's results. */
+int cbp_server_release(cbp_server* server, uint64_t ticket);
+/* Finish the queued requests, stop the threads, free everything. */
+int cbp_server_destroy(cbp_server* server);
+/* Message of the last failed server call on the calling thread. */
+const char* cbp_server_last_error(void);
+
 /* Limit the number of database positions processed per slab (0 = plan by
  * the memory budget). Used to exercise multi-slab processing. */
 int cbp_set_max_slab_positions(cbp_context* ctx, size_t max_positions);
