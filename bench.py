@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--cvswgt", type=float, default=0.0,
                     help="weight of the context-vector term (0 = off, the parity configuration; "
                          "the reference's own default is 0.15); > 0 gives the profiles context vectors")
+    ap.add_argument("--ddmswgt", type=float, default=0.2,
+                    help="weight of the DDMS term (the parity configuration's 0.2; 0 leaves the "
+                         "profile-profile and SS terms, and the phase-1 DP dominates)")
     ap.add_argument("--serve", action="store_true",
                     help="request loop over a resident database: queries/s and p50/p99 latency")
     ap.add_argument("--rate", default="5", help="--serve: offered loads (Poisson, queries/s), comma list")
@@ -238,7 +241,8 @@ def workload_config(args, q, db, world: int) -> dict:
     """The `config` of the JSON line: the same for both arms."""
     return {"workload": args.workload, "query_len": q.npositions, "db_profiles": db.nprofiles,
             "db_positions": db.npositions, "stages": STAGES, "tc_form": args.tc,
-            "cvswgt": args.cvswgt, "l2": "inputs larger than L2 (database chunk > 126 MB)",
+            "cvswgt": args.cvswgt, "ddmswgt": args.ddmswgt,
+            "l2": "inputs larger than L2 (database chunk > 126 MB)",
             "parallelism": f"dp{world} (database shard per GPU)"}
 
 
@@ -382,6 +386,9 @@ def main():
     opts = cb.Options.defaults()
     opts.tc_form = {"plain": cb.TC_PLAIN, "bf16": cb.TC_BF16X3, "tf32": cb.TC_TF32X3}[args.tc]
     opts.cvswgt = args.cvswgt
+    opts.ddmswgt = args.ddmswgt
+    if args.ddmswgt <= 0:
+        steps_ddms = 0
     bp = cb.BatchProcessing(ss, opts, device=local)
     if args.cvswgt > 0:
         cvs = np.load(os.path.join(ROOT, "tests", "golden", "cvs2s.npz"))
@@ -446,11 +453,11 @@ def main():
         peaks = measured_peaks()
         rows = bp.tuning(Lq)["score_rows"]
         score_launch_ms = score_ms / max(1, score_launches)
+        sm_mhz = clocks.get("sm_max_mhz") or 1965.0
+        alu_peak = 148 * 128 * sm_mhz * 1e6 / 1e9  # lane-ops/s at max clock, Gop/s
         # one launch per slab; the workload here fits one slab
         ops = steps_ddms * OPS_PER_DDMS_STEP * args.steps / max(1, score_launches)
         achieved = ops / (score_launch_ms / 1e3) / 1e9  # Gop/s
-        sm_mhz = clocks.get("sm_max_mhz") or 1965.0
-        alu_peak = 148 * 128 * sm_mhz * 1e6 / 1e9  # lane-ops/s at max clock, Gop/s
         roof = {"bound": "alu", "achieved": achieved, "peak": alu_peak, "unit": "Gop/s",
                 "frac": achieved / alu_peak,
                 "traffic": score_traffic_per_cell(rows) * float(Lq) * Ndb,
@@ -463,6 +470,16 @@ def main():
                 "peak_source": "148 SMs x 128 FP32 lanes x max SM clock (nominal issue rate)",
                 "hbm_bytes_per_launch": float(Lq) * Ndb * 8,
                 "hbm_peak_gbs": (peaks or {}).get("hbm_gbs")}
+        if args.ddmswgt <= 0:
+            # without DDMS the phase-1 DP dominates: its ALU roofline at 37
+            # algorithmic ops per cell (SURVEY's count for the 5-state DP)
+            dp_ms = stage_acc[1] / steps
+            achieved = 37.0 * Lq * Ndb / (dp_ms / 1e3) / 1e9
+            roof = {"bound": "alu", "achieved": achieved, "peak": alu_peak, "unit": "Gop/s",
+                    "frac": achieved / alu_peak, "traffic": None, "kernel": "dp1_kernel",
+                    "peak_source": "148 SMs x 128 FP32 lanes x max SM clock (nominal issue rate)",
+                    "hbm_bytes_per_launch": float(Lq) * Ndb * 5,
+                    "hbm_peak_gbs": (peaks or {}).get("hbm_gbs")}
         line = {"metric": "GCUPS", "value": value, "unit": "GCUPS", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": kern_ms / steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

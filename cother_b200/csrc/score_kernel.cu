@@ -241,8 +241,10 @@ __device__ __forceinline__ float cvs_cell(const ScoreArgs& a, const float* __res
 }
 
 // kRows query positions per block (8, 16 or 32; each warp takes every
-// kWarps-th of them), chosen by the tuner
-template <int kRows>
+// kWarps-th of them), chosen by the tuner. kStacked: the rows belong to
+// several queries (cbp_process_batch), each with its own background; a
+// separate instantiation, so that the single-query kernel is unchanged.
+template <int kRows, bool kStacked>
 __global__ void __launch_bounds__(kThreads, 10)
 score_matrix_kernel(const ScoreArgs a)
 {
@@ -375,7 +377,7 @@ score_matrix_kernel(const ScoreArgs a)
         float acc = 0.0f;
         if (a.dots_in_scores) {
             acc = a.scores[(long long)row * a.ld + col];
-        } else if (a.q.P == 1) {
+        } else if (!kStacked) {
 #pragma unroll
             for (int k = 0; k < kNAA; k++) {
                 const float num = s_qtf[r][k] * s_dtf[k][lane];
@@ -513,7 +515,8 @@ void launch_score_rows(const ScoreArgs& a, cudaStream_t stream)
     dim3 grid((unsigned)ceil_div(a.ncols, kCols), (unsigned)ceil_div(a.Lq, kRows));
     const size_t cvs_smem =
         a.cvswgt > 0.0f ? sizeof(float) * ((kNCV + 2) * kCols + kRows * (kNCV + 1) + 2 * kRows) : 0;
-    score_matrix_kernel<kRows><<<grid, kThreads, cvs_smem, stream>>>(a);
+    if (a.q.P > 1) score_matrix_kernel<kRows, true><<<grid, kThreads, cvs_smem, stream>>>(a);
+    else score_matrix_kernel<kRows, false><<<grid, kThreads, cvs_smem, stream>>>(a);
     CBP_CHECK_LAUNCH();
 }
 
