@@ -560,8 +560,9 @@ void tune_kernels(cbp_context* c, const ScoreArgs& base, int p0, int p1, Tuning&
     for (int k = 0; k < kScoreCandidates; k++) {
         a.rows = kScoreRowsCand[k];
         t.score_ms[k] = time_it([&] {
-            launch_column_order(db.view.dstlen, a.col0, a.ncols, a.ld, kWindowCand[k], c->colorder.as<int>(),
-                                c->stream);
+            if (a.colorder)
+                launch_column_order(db.view.dstlen, a.col0, a.ncols, a.ld, kWindowCand[k], c->colorder.as<int>(),
+                                    c->stream);
             launch_score_matrix(a, c->stream);
         });
         c->launches += 4;
@@ -776,7 +777,9 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
         a.dmstab = c->dmstab.as<float>();
         a.scores = c->scores.as<float>();
         a.modscores = c->modscores.as<float>();
-        a.colorder = c->colorder.as<int>();
+        // the column order only balances the DDMS loops of a warp's lanes;
+        // without that term the identity keeps the stores coalesced
+        a.colorder = a.ddmswgt > 0.0f ? c->colorder.as<int>() : nullptr;
         Tuning& tn = c->tuning[Ltot / 64];
         if (c->opt.autotune && !tn.tuned) tune_kernels(c, a, s.p0, s.p1, tn);
         a.rows = tn.rows;
@@ -844,8 +847,9 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
                 else CBP_CUDA(cudaEventRecord(e, c->stream));
             };
             if (!tc) mark(c->ev[0]);
-            launch_column_order(c->db->view.dstlen, s.col0, s.ncols, a.ld, tn.window, c->colorder.as<int>(),
-                                c->stream);
+            if (a.colorder)
+                launch_column_order(c->db->view.dstlen, s.col0, s.ncols, a.ld, tn.window, c->colorder.as<int>(),
+                                    c->stream);
             launch_score_matrix(a, c->stream);
             mark(c->ev[1]);
             CBP_CUDA(cudaMemsetAsync(c->dp1err.p, 0, sizeof(int), c->stream));

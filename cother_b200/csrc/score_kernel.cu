@@ -257,7 +257,6 @@ score_matrix_kernel(const ScoreArgs a)
     __shared__ float s_dss[kNSS][kCols];
     __shared__ float s_qtf[kRows][kNAA + 1];
     __shared__ float s_qss[kRows][kNSS];
-    __shared__ float s_qbg[kNAA];
     __shared__ int s_dlen[kCols];
     __shared__ int s_qlen[kRows];
     // context vectors and their log priors and squared norms (CVSWGT > 0):
@@ -281,7 +280,7 @@ score_matrix_kernel(const ScoreArgs a)
         const int slot = colb + tid;
         s_col[tid] = slot < a.ncols ? (a.colorder ? a.colorder[slot] : slot) : -1;
     }
-    for (int i = tid; i < kDstCard * kDstCard; i += kThreads) s_dms[i] = a.dmstab[i] * 0x1p-7f;
+    for (int i = tid; a.ddmswgt > 0.0f && i < kDstCard * kDstCard; i += kThreads) s_dms[i] = a.dmstab[i] * 0x1p-7f;
     for (int i = tid; i < kSSCard * kSSCard; i += kThreads) s_sst[i] = a.sstab[i];
     __syncthreads();
 
@@ -293,7 +292,11 @@ score_matrix_kernel(const ScoreArgs a)
         const int p = a.db.pro[gpos];
         for (int k = warp; k < kNAA; k += kWarps) {
             s_dtf[k][lane] = a.db.tf[(long long)k * N + gpos];
-            s_dbg[k][lane] = a.db.bkg[(long long)k * a.db.P + p];
+            // one query: the denominator 0.5*(query bkg + profile bkg) of
+            // the column, rounded as in the cell loop; stacked queries: the
+            // profile's background alone
+            const float b = a.db.bkg[(long long)k * a.db.P + p];
+            s_dbg[k][lane] = kStacked ? b : 0.5f * (__ldg(a.q.bkg + k) + b);
         }
         if (warp < kNSS) s_dss[warp][lane] = a.db.ss[(long long)warp * N + gpos];
         if (warp == kNSS) s_dlen[lane] = a.db.dstlen[gpos];
@@ -302,8 +305,9 @@ score_matrix_kernel(const ScoreArgs a)
     }
     // distance lists: 32 columns x 104 bytes, in 16-byte pieces, each code
     // times 4 (a byte offset in a row of the pair-score table; codes <= 21,
-    // so the shift never carries across bytes)
-    for (int idx = tid; idx < kCols * 7; idx += kThreads) {
+    // so the shift never carries across bytes); only for the DDMS term
+    const bool ddms = a.ddmswgt > 0.0f;
+    for (int idx = tid; ddms && idx < kCols * 7; idx += kThreads) {
         const int c = idx / 7, piece = idx - c * 7;
         const int cc = s_col[c];
         uint4 v;
@@ -347,10 +351,9 @@ score_matrix_kernel(const ScoreArgs a)
             s_qcvpn[1][tid] = row < a.Lq ? a.q.cvnorm2[row] : 0.0f;
         }
     }
-    if (tid < kNAA) s_qbg[tid] = a.q.bkg[tid];
     if (tid < kRows) s_qlen[tid] = (rowb + tid < a.Lq) ? a.q.dstlen[rowb + tid] : 0;
     // query lists: each code times 88, the byte offset of its table row
-    for (int idx = tid; idx < kRows * (kElems / 4); idx += kThreads) {
+    for (int idx = tid; ddms && idx < kRows * (kElems / 4); idx += kThreads) {
         const int r = idx / (kElems / 4), w = idx - r * (kElems / 4);
         const int row = rowb + r;
         uint32_t v = 0x15151515u;
@@ -381,8 +384,7 @@ score_matrix_kernel(const ScoreArgs a)
 #pragma unroll
             for (int k = 0; k < kNAA; k++) {
                 const float num = s_qtf[r][k] * s_dtf[k][lane];
-                const float den = 0.5f * (s_qbg[k] + s_dbg[k][lane]);
-                acc = acc + __fdiv_rn(num, den);
+                acc = acc + __fdiv_rn(num, s_dbg[k][lane]);
             }
         } else {
             // stacked queries: the background of this row's query
