@@ -45,7 +45,7 @@ class Options(ctypes.Structure):
         ("dstsegm", ctypes.c_int), ("mapaln", ctypes.c_int), ("minpp", ctypes.c_float),
         ("ssemodel", ctypes.c_int), ("x_uninf", ctypes.c_int), ("eval", ctypes.c_float),
         ("nohits", ctypes.c_int), ("noalns", ctypes.c_int), ("tc_form", ctypes.c_int),
-        ("autotune", ctypes.c_int),
+        ("autotune", ctypes.c_int), ("all_codes", ctypes.c_int),
     ]
 
     @classmethod

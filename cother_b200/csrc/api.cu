@@ -828,6 +828,8 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
             d[k].bandbuf = c->bandbuf.as<float>();
             d[k].maxsc = c->dpmax.as<float>() + k * maxprof;
             d[k].maxcoords = c->dpcoords.as<uint32_t>() + k * maxprof;
+            // codes for the finalization's candidates only, unless all are asked for
+            d[k].code_thld = c->opt.all_codes ? -INFINITY : r.score_thld;
             d[k].recs = c->dprecs.as<Dp1Rec>() + k * maxprof;
             d[k].warps = tn.dp_warps;
             d[k].err = c->dp1err.as<int>();
@@ -1122,6 +1124,7 @@ void cbp_default_options(cbp_options* o)
     o->noalns = 700;
     o->tc_form = CBP_TC_PLAIN;
     o->autotune = 1;
+    o->all_codes = 0;
 }
 
 const char* cbp_last_error(void) { return g_last_error.c_str(); }

@@ -171,6 +171,20 @@ __device__ __forceinline__ int dp_cell(const S5& d, const S5& u, const S5& l, co
     return (n.MM == M) ? bmm : bud;
 }
 
+// The states of one cell alone (a sweep without backtrack codes).
+__device__ __forceinline__ void dp_states(const S5& d, const S5& u, const S5& l, const Q7& q, const Q7& t,
+                                          float sc, S5& n)
+{
+    const float m1 = fmaxf(d.MI + q.MM + t.IM, d.IM + q.IM + t.MM);
+    const float m2 = fmaxf(d.DN + q.DM + t.MM, d.ND + q.MM + t.DM);
+    const float m3 = fmaxf(m1, fmaxf(m2, d.MM + q.MM + t.MM));
+    n.MM = fmaxf(m3 + sc, 0.0f);
+    n.MI = fmaxf(u.MM + q.MM + t.MIc, u.MI + q.MM + t.IIc);
+    n.IM = fmaxf(l.MM + q.MIc + t.MM, l.IM + q.IIc + t.MM);
+    n.DN = fmaxf(u.MM + q.MD, u.DN + q.DD);
+    n.ND = fmaxf(l.MM + t.MD, l.ND + t.DD);
+}
+
 __device__ __forceinline__ Q7 query_trn(const float* __restrict__ qtrn, long long QT, int r, int Lq)
 {
     Q7 q;
@@ -237,258 +251,293 @@ dp1_kernel(const Dp1Args a)
     float best = 0.0f;
     int bestr = 0, bestc = 0;
 
-    for (int r0 = 0; r0 < Lq && ok; r0 += kBand) {
-        const int rA = r0 + 2 * lane, rB = rA + 1;
-        const bool vA = rA < Lq, vB = rB < Lq;
-        const Q7 qa = query_trn(a.qtrn, QT, rA, Lq);
-        const Q7 qb = query_trn(a.qtrn, QT, rB, Lq);
-        const bool top = (r0 == 0);
-        const bool has_next = r0 + kBand < Lq;
-        const bool full = r0 + kBand <= Lq;           // all 64 rows exist
-        const int nlanes = min(32, (Lq - r0 + 1) >> 1);   // lanes holding a row
-        const int nsteps = Ld + nlanes - 1;
-        const bool lastB = (rB & 31) == 31;  // the last row of a 32-row band of the reference
-        // column -1 of each row, as the reference's block schedule leaves
-        // it (CuBatchDP_init_btck.cu:93-160, 190-300): MM = 0, MI = IM = ND
-        // ~ -32768 and DN(r) = max(qMD(r), DN(r-1) + qDD(r)), from
-        // max(qMD, qDD) on a 32-row band's first row; a 32-row band's last
-        // row starts at column 0 from zeroed predecessors
-        float dnA = 0.0f, dnB = 0.0f;
-        for (int k = 0; k < 16; k++) {
-            const float up = __shfl_up_sync(kFull, dnB, 1);
-            if ((lane & 15) == k) {
-                dnA = (k == 0) ? hmax(0.0f + qa.MD, 0.0f + qa.DD) : hmax(0.0f + qa.MD, up + qa.DD);
-                dnB = hmax(0.0f + qb.MD, dnA + qb.DD);
-            }
-        }
-        S5 lA = {0.0f, kLog0, kLog0, dnA, kLog0};
-        S5 lB = lastB ? S5{0.0f, 0.0f, 0.0f, 0.0f, 0.0f} : S5{0.0f, kLog0, kLog0, dnB, kLog0};
-        S5 dg = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};       // row A's diagonal: the previous step's up
-        // corner triangles (ExecDP_Btck_Unroll32x excludes them): a cell is
-        // in a corner when c <= ca or c >= cb for its row
-        const bool bcorner = (r0 < edge) || (r0 + kBand - 1 + edge >= Lq);
-        const int caA = (Lq <= rA + edge) ? edge + rA - Lq : -1;
-        const int cbA = (rA < edge) ? Ld - edge + rA : 0x7fffffff;
-        const int caB = (Lq <= rB + edge) ? edge + rB - Lq : -1;
-        const int cbB = (rB < edge) ? Ld - edge + rB : 0x7fffffff;
-        float bstA = 0.0f, bstB = 0.0f;
-        int bcA = 0, bcB = 0;
-
-        // fetch piece h of this band into ring slot h mod 4
-        auto issue = [&](int h) {
-            const int slot = h & (kSlots - 1);
-            const int c0 = kPiece * h - off;            // first column of the piece
-            if (kBulk) {
-                const int ncol = min(kPiece, Ld - c0);   // >= 1: h <= h_last
-                const unsigned bytes = (unsigned)((ncol * 4 + 15) & ~15);
-                const int nrows = min(kBand, Lq - r0);
-                if (lane == 0) mbar_expect_tx(&st.bar[slot], bytes * (unsigned)nrows);
-                __syncwarp();
-                // the slot's earlier contents were read through the generic
-                // proxy; order those reads before the bulk copy's writes
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                if (vA) bulk_load(&st.sc[2 * lane][kPiece * slot], S + (long long)rA * ld + c0, bytes, &st.bar[slot]);
-                if (vB) bulk_load(&st.sc[2 * lane + 1][kPiece * slot], S + (long long)rB * ld + c0, bytes,
-                                  &st.bar[slot]);
-            } else {
-#pragma unroll 4
-                for (int j = 0; j < kPiece; j++) {
-                    const int c = c0 + j;
-                    const bool cv = c < Ld;
-                    cp_async4(&st.sc[2 * lane][kPiece * slot + j], (vA && cv) ? S + (long long)rA * ld + c : S,
-                              vA && cv);
-                    cp_async4(&st.sc[2 * lane + 1][kPiece * slot + j], (vB && cv) ? S + (long long)rB * ld + c : S,
-                              vB && cv);
+    using kTrue = std::integral_constant<bool, true>;
+    using kFalse = std::integral_constant<bool, false>;
+    // One sweep over the profile's DP. kCodes: with the backtrack codes and
+    // the coordinates of the maximum; without them, the maximum alone.
+    auto sweep = [&](auto codes_tag) {
+        constexpr bool kCodes = decltype(codes_tag)::value;
+        best = 0.0f;
+        bestr = 0;
+        bestc = 0;
+        for (int r0 = 0; r0 < Lq && ok; r0 += kBand) {
+            const int rA = r0 + 2 * lane, rB = rA + 1;
+            const bool vA = rA < Lq, vB = rB < Lq;
+            const Q7 qa = query_trn(a.qtrn, QT, rA, Lq);
+            const Q7 qb = query_trn(a.qtrn, QT, rB, Lq);
+            const bool top = (r0 == 0);
+            const bool has_next = r0 + kBand < Lq;
+            const bool full = r0 + kBand <= Lq;           // all 64 rows exist
+            const int nlanes = min(32, (Lq - r0 + 1) >> 1);   // lanes holding a row
+            const int nsteps = Ld + nlanes - 1;
+            const bool lastB = (rB & 31) == 31;  // the last row of a 32-row band of the reference
+            // column -1 of each row, as the reference's block schedule leaves
+            // it (CuBatchDP_init_btck.cu:93-160, 190-300): MM = 0, MI = IM = ND
+            // ~ -32768 and DN(r) = max(qMD(r), DN(r-1) + qDD(r)), from
+            // max(qMD, qDD) on a 32-row band's first row; a 32-row band's last
+            // row starts at column 0 from zeroed predecessors
+            float dnA = 0.0f, dnB = 0.0f;
+            for (int k = 0; k < 16; k++) {
+                const float up = __shfl_up_sync(kFull, dnB, 1);
+                if ((lane & 15) == k) {
+                    dnA = (k == 0) ? hmax(0.0f + qa.MD, 0.0f + qa.DD) : hmax(0.0f + qa.MD, up + qa.DD);
+                    dnB = hmax(0.0f + qb.MD, dnA + qb.DD);
                 }
             }
-            const int j = lane & 15;
-            const int c = c0 + j;
-            const bool cv = c >= 0 && c < Ld;
-            const bool sv = cv && !top;                 // the strip: zeros on the first band
-            const int pos = kPiece * slot + j;
-            if (lane < 16) {
-                float* d = reinterpret_cast<float*>(&st.tra[pos]);
-                cp_async4(d + 0, cv ? trn + trMM * NT + tb + c : trn, cv);
-                cp_async4(d + 1, cv ? trn + trIM * NT + tb + c : trn, cv);
-                cp_async4(d + 2, cv ? trn + trDM * NT + tb + c : trn, cv);
-                cp_async4(d + 3, cv ? trn + trMD * NT + tb + c : trn, cv);
-                float* e = reinterpret_cast<float*>(&st.spa[pos]);
-                cp_async4(e + 0, sv ? strip + 0 * ld + c : trn, sv);
-                cp_async4(e + 1, sv ? strip + 1 * ld + c : trn, sv);
-            } else {
-                float* d = reinterpret_cast<float*>(&st.trb[pos]);
-                cp_async4(d + 0, cv ? trn + trDD * NT + tb + c : trn, cv);
-                cp_async4(d + 1, cv ? trn + trMI * NT + tb + c + 1 : trn, cv);
-                cp_async4(d + 2, cv ? trn + trII * NT + tb + c + 1 : trn, cv);
-                float* e = reinterpret_cast<float*>(&st.spa[pos]);
-                cp_async4(e + 2, sv ? strip + 2 * ld + c : trn, sv);
-                cp_async4(e + 3, sv ? strip + 3 * ld + c : trn, sv);
-                cp_async4(&st.spb[pos], sv ? strip + 4 * ld + c : trn, sv);
-            }
-            cp_async_commit();
-        };
-        // wait until piece h is resident (piece h+1 in flight when `more`);
-        // false if its score rows never arrived, after a bounded wait for
-        // the copies still in flight into this warp's shared memory
-        auto await = [&](int h, bool more) {
-            cp_async_wait1();
-            if (!kBulk) {
-                __syncwarp();
-                return true;
-            }
-            const int slot = h & (kSlots - 1);
-            const unsigned par = (phases >> slot) & 1u;
-            const bool got = __all_sync(kFull, mbar_wait(&st.bar[slot], par));
-            if (got) {
-                phases ^= 1u << slot;
-                __syncwarp();
-                return true;
-            }
-            cp_async_wait0();
-            (void)mbar_wait(&st.bar[slot], par);
-            if (more) {
-                const int s1 = (h + 1) & (kSlots - 1);
-                (void)mbar_wait(&st.bar[s1], (phases >> s1) & 1u);
-            }
-            return false;
-        };
-        // write back piece h (lane 31 has left it): the backtrack codes of
-        // its columns inside the profile, and the band's bottom row
-        auto flush = [&](int h) {
-            const int slot = h & (kSlots - 1);
-            const int c0 = kPiece * h - off;
-            const uint4 pk = *reinterpret_cast<const uint4*>(&st.bt[lane][kPiece * slot]);
-            const uint32_t pw[4] = {pk.x, pk.y, pk.z, pk.w};
+            S5 lA = {0.0f, kLog0, kLog0, dnA, kLog0};
+            S5 lB = lastB ? S5{0.0f, 0.0f, 0.0f, 0.0f, 0.0f} : S5{0.0f, kLog0, kLog0, dnB, kLog0};
+            S5 dg = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};       // row A's diagonal: the previous step's up
+            // corner triangles (ExecDP_Btck_Unroll32x excludes them): a cell is
+            // in a corner when c <= ca or c >= cb for its row
+            const bool bcorner = (r0 < edge) || (r0 + kBand - 1 + edge >= Lq);
+            const int caA = (Lq <= rA + edge) ? edge + rA - Lq : -1;
+            const int cbA = (rA < edge) ? Ld - edge + rA : 0x7fffffff;
+            const int caB = (Lq <= rB + edge) ? edge + rB - Lq : -1;
+            const int cbB = (rB < edge) ? Ld - edge + rB : 0x7fffffff;
+            float bstA = 0.0f, bstB = 0.0f;
+            int bcA = 0, bcB = 0;
+
+            // fetch piece h of this band into ring slot h mod 4
+            auto issue = [&](int h) {
+                const int slot = h & (kSlots - 1);
+                const int c0 = kPiece * h - off;            // first column of the piece
+                if (kBulk) {
+                    const int ncol = min(kPiece, Ld - c0);   // >= 1: h <= h_last
+                    const unsigned bytes = (unsigned)((ncol * 4 + 15) & ~15);
+                    const int nrows = min(kBand, Lq - r0);
+                    if (lane == 0) mbar_expect_tx(&st.bar[slot], bytes * (unsigned)nrows);
+                    __syncwarp();
+                    // the slot's earlier contents were read through the generic
+                    // proxy; order those reads before the bulk copy's writes
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    if (vA) bulk_load(&st.sc[2 * lane][kPiece * slot], S + (long long)rA * ld + c0, bytes, &st.bar[slot]);
+                    if (vB) bulk_load(&st.sc[2 * lane + 1][kPiece * slot], S + (long long)rB * ld + c0, bytes,
+                                      &st.bar[slot]);
+                } else {
+#pragma unroll 4
+                    for (int j = 0; j < kPiece; j++) {
+                        const int c = c0 + j;
+                        const bool cv = c < Ld;
+                        cp_async4(&st.sc[2 * lane][kPiece * slot + j], (vA && cv) ? S + (long long)rA * ld + c : S,
+                                  vA && cv);
+                        cp_async4(&st.sc[2 * lane + 1][kPiece * slot + j], (vB && cv) ? S + (long long)rB * ld + c : S,
+                                  vB && cv);
+                    }
+                }
+                const int j = lane & 15;
+                const int c = c0 + j;
+                const bool cv = c >= 0 && c < Ld;
+                const bool sv = cv && !top;                 // the strip: zeros on the first band
+                const int pos = kPiece * slot + j;
+                if (lane < 16) {
+                    float* d = reinterpret_cast<float*>(&st.tra[pos]);
+                    cp_async4(d + 0, cv ? trn + trMM * NT + tb + c : trn, cv);
+                    cp_async4(d + 1, cv ? trn + trIM * NT + tb + c : trn, cv);
+                    cp_async4(d + 2, cv ? trn + trDM * NT + tb + c : trn, cv);
+                    cp_async4(d + 3, cv ? trn + trMD * NT + tb + c : trn, cv);
+                    float* e = reinterpret_cast<float*>(&st.spa[pos]);
+                    cp_async4(e + 0, sv ? strip + 0 * ld + c : trn, sv);
+                    cp_async4(e + 1, sv ? strip + 1 * ld + c : trn, sv);
+                } else {
+                    float* d = reinterpret_cast<float*>(&st.trb[pos]);
+                    cp_async4(d + 0, cv ? trn + trDD * NT + tb + c : trn, cv);
+                    cp_async4(d + 1, cv ? trn + trMI * NT + tb + c + 1 : trn, cv);
+                    cp_async4(d + 2, cv ? trn + trII * NT + tb + c + 1 : trn, cv);
+                    float* e = reinterpret_cast<float*>(&st.spa[pos]);
+                    cp_async4(e + 2, sv ? strip + 2 * ld + c : trn, sv);
+                    cp_async4(e + 3, sv ? strip + 3 * ld + c : trn, sv);
+                    cp_async4(&st.spb[pos], sv ? strip + 4 * ld + c : trn, sv);
+                }
+                cp_async_commit();
+            };
+            // wait until piece h is resident (piece h+1 in flight when `more`);
+            // false if its score rows never arrived, after a bounded wait for
+            // the copies still in flight into this warp's shared memory
+            auto await = [&](int h, bool more) {
+                cp_async_wait1();
+                if (!kBulk) {
+                    __syncwarp();
+                    return true;
+                }
+                const int slot = h & (kSlots - 1);
+                const unsigned par = (phases >> slot) & 1u;
+                const bool got = __all_sync(kFull, mbar_wait(&st.bar[slot], par));
+                if (got) {
+                    phases ^= 1u << slot;
+                    __syncwarp();
+                    return true;
+                }
+                cp_async_wait0();
+                (void)mbar_wait(&st.bar[slot], par);
+                if (more) {
+                    const int s1 = (h + 1) & (kSlots - 1);
+                    (void)mbar_wait(&st.bar[s1], (phases >> s1) & 1u);
+                }
+                return false;
+            };
+            // write back piece h (lane 31 has left it): the backtrack codes of
+            // its columns inside the profile, and the band's bottom row
+            auto flush = [&](int h) {
+                const int slot = h & (kSlots - 1);
+                const int c0 = kPiece * h - off;
+                const uint4 pk = *reinterpret_cast<const uint4*>(&st.bt[lane][kPiece * slot]);
+                const uint32_t pw[4] = {pk.x, pk.y, pk.z, pk.w};
 #pragma unroll
-            for (int k = 0; k < 2; k++) {
-                if (r0 + 2 * lane + k >= Lq) continue;
-                uint8_t* dst = B + (long long)(r0 + 2 * lane + k) * ld + c0;
+                for (int k = 0; k < 2; k++) {
+                    if (!kCodes || r0 + 2 * lane + k >= Lq) continue;
+                    uint8_t* dst = B + (long long)(r0 + 2 * lane + k) * ld + c0;
 #pragma unroll
-                for (int wd = 0; wd < 4; wd++) {
-                    const uint32_t v = (pw[wd] >> (4 * k)) & 0x0f0f0f0fu;
-                    const int cw = c0 + 4 * wd;
-                    if (kBulk && cw >= 0 && cw + 4 <= Ld) {
-                        *reinterpret_cast<uint32_t*>(dst + 4 * wd) = v;
-                    } else {
-                        for (int i = 0; i < 4; i++) {
-                            const int cc = cw + i;
-                            if (cc >= 0 && cc < Ld) dst[4 * wd + i] = (uint8_t)(v >> (8 * i));
+                    for (int wd = 0; wd < 4; wd++) {
+                        const uint32_t v = (pw[wd] >> (4 * k)) & 0x0f0f0f0fu;
+                        const int cw = c0 + 4 * wd;
+                        if (kBulk && cw >= 0 && cw + 4 <= Ld) {
+                            *reinterpret_cast<uint32_t*>(dst + 4 * wd) = v;
+                        } else {
+                            for (int i = 0; i < 4; i++) {
+                                const int cc = cw + i;
+                                if (cc >= 0 && cc < Ld) dst[4 * wd + i] = (uint8_t)(v >> (8 * i));
+                            }
                         }
                     }
                 }
-            }
-            if (has_next && lane < kPiece) {
-                const int c = c0 + lane;
-                if (c >= 0 && c < Ld) {
-                    const float4 v = st.soa[kPiece * slot + lane];
-                    strip[0 * ld + c] = v.x; strip[1 * ld + c] = v.y; strip[2 * ld + c] = v.z;
-                    strip[3 * ld + c] = v.w; strip[4 * ld + c] = st.sob[kPiece * slot + lane];
-                }
-            }
-        };
-
-        // one step: cells (rA, c) and (rB, c) of the lane, c = s - lane.
-        // kChecked: some lane may be outside the profile or below the last
-        // row, or at column 0; kCorner: the band reaches a corner triangle
-        auto step = [&](int s, auto checked_tag, auto corner_tag) {
-            constexpr bool kChecked = decltype(checked_tag)::value;
-            constexpr bool kCorner = decltype(corner_tag)::value;
-            const int c = s - lane;
-            S5 u;
-            u.MM = __shfl_up_sync(kFull, lB.MM, 1);
-            u.MI = __shfl_up_sync(kFull, lB.MI, 1);
-            u.IM = __shfl_up_sync(kFull, lB.IM, 1);
-            u.DN = __shfl_up_sync(kFull, lB.DN, 1);
-            u.ND = __shfl_up_sync(kFull, lB.ND, 1);
-            const int pos = (c + off) & (kRing - 1);
-            {
-                // lane 0: the previous band's bottom row (zeros on the first
-                // band and outside the profile)
-                const float4 v = st.spa[pos];
-                const float w = st.spb[pos];
-                if (lane == 0) { u.MM = v.x; u.MI = v.y; u.IM = v.z; u.DN = v.w; u.ND = w; }
-            }
-            bool doA = true, doB = true;
-            if (kChecked) {
-                doA = vA && c >= 0 && c < Ld;
-                doB = doA && vB;
-            }
-            if (doA) {
-                const float4 ta = st.tra[pos];
-                const float4 tc = st.trb[pos];
-                Q7 t;
-                t.MM = ta.x; t.IM = ta.y; t.DM = ta.z; t.MD = ta.w;
-                t.DD = tc.x; t.MIc = tc.y; t.IIc = tc.z;
-                float scA = st.sc[2 * lane][pos];
-                if (kCorner && (c <= caA || c >= cbA)) scA = -9.0f;
-                S5 nA;
-                int code = dp_cell(dg, u, lA, qa, t, scA, nA);
-                if (bstA < nA.MM) { bstA = nA.MM; bcA = c; }
-                if (doB) {
-                    float scB = st.sc[2 * lane + 1][pos];
-                    if (kCorner && (c <= caB || c >= cbB)) scB = -9.0f;
-                    // diagonal of (rB, c) = (rA, c-1): row A's left state; a
-                    // 32-row band's last row takes zeros at column 0
-                    S5 dB = lA;
-                    if (kChecked && lastB && c == 0) dB = S5{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-                    S5 nB;
-                    code |= dp_cell(dB, nA, lB, qb, t, scB, nB) << 4;
-                    if (bstB < nB.MM) { bstB = nB.MM; bcB = c; }
-                    lB = nB;
-                    if (lane == 31) {
-                        st.soa[pos] = make_float4(nB.MM, nB.MI, nB.IM, nB.DN);
-                        st.sob[pos] = nB.ND;
+                if (has_next && lane < kPiece) {
+                    const int c = c0 + lane;
+                    if (c >= 0 && c < Ld) {
+                        const float4 v = st.soa[kPiece * slot + lane];
+                        strip[0 * ld + c] = v.x; strip[1 * ld + c] = v.y; strip[2 * ld + c] = v.z;
+                        strip[3 * ld + c] = v.w; strip[4 * ld + c] = st.sob[kPiece * slot + lane];
                     }
                 }
-                st.bt[lane][pos] = (uint8_t)code;
-                lA = nA;
-            }
-            dg = u;
-        };
-        using kTrue = std::integral_constant<bool, true>;
-        using kFalse = std::integral_constant<bool, false>;
+            };
 
-        __syncwarp();   // the previous band's tiles are no longer read
-        issue(0);
-        int hflushed = 0;   // pieces 0 .. hflushed-1 are written back
-        // steps with every lane inside the profile and on a row (the
-        // unchecked steps): [32, Ld) on a full band
-        const int fast0 = full ? 32 : nsteps, fast1 = full ? Ld : nsteps;
-        for (int H = 0;; H++) {
-            const int sb = (H == 0) ? 0 : kPiece * H - off;   // lane 0 enters piece H
-            if (sb >= nsteps) break;
-            const int se = min(kPiece * H + kPiece - off, nsteps);
-            __syncwarp();
-            // lane 31 left piece H-3 two steps ago; its ring slot takes piece H+1
-            if (H >= 3 && H - 3 <= h_last) { flush(H - 3); hflushed = H - 2; }
-            if (H <= h_last) {
-                const bool more = H + 1 <= h_last;
-                if (more) issue(H + 1);
-                else cp_async_commit();   // an empty group keeps the wait accounting
-                if (!await(H, more)) { ok = false; break; }
-            }
-            const int f0 = max(sb, fast0), f1 = min(se, fast1);
-            if (f0 < f1) {
-                for (int s = sb; s < f0; s++) step(s, kTrue(), kTrue());
-                if (bcorner) {
-#pragma unroll 2
-                    for (int s = f0; s < f1; s++) step(s, kFalse(), kTrue());
-                } else {
-#pragma unroll 2
-                    for (int s = f0; s < f1; s++) step(s, kFalse(), kFalse());
+            // one step: cells (rA, c) and (rB, c) of the lane, c = s - lane.
+            // kChecked: some lane may be outside the profile or below the last
+            // row, or at column 0; kCorner: the band reaches a corner triangle
+            auto step = [&](int s, auto checked_tag, auto corner_tag) {
+                constexpr bool kChecked = decltype(checked_tag)::value;
+                constexpr bool kCorner = decltype(corner_tag)::value;
+                const int c = s - lane;
+                S5 u;
+                u.MM = __shfl_up_sync(kFull, lB.MM, 1);
+                u.MI = __shfl_up_sync(kFull, lB.MI, 1);
+                u.IM = __shfl_up_sync(kFull, lB.IM, 1);
+                u.DN = __shfl_up_sync(kFull, lB.DN, 1);
+                u.ND = __shfl_up_sync(kFull, lB.ND, 1);
+                const int pos = (c + off) & (kRing - 1);
+                {
+                    // lane 0: the previous band's bottom row (zeros on the first
+                    // band and outside the profile)
+                    const float4 v = st.spa[pos];
+                    const float w = st.spb[pos];
+                    if (lane == 0) { u.MM = v.x; u.MI = v.y; u.IM = v.z; u.DN = v.w; u.ND = w; }
                 }
-                for (int s = f1; s < se; s++) step(s, kTrue(), kTrue());
+                bool doA = true, doB = true;
+                if (kChecked) {
+                    doA = vA && c >= 0 && c < Ld;
+                    doB = doA && vB;
+                }
+                if (doA) {
+                    const float4 ta = st.tra[pos];
+                    const float4 tc = st.trb[pos];
+                    Q7 t;
+                    t.MM = ta.x; t.IM = ta.y; t.DM = ta.z; t.MD = ta.w;
+                    t.DD = tc.x; t.MIc = tc.y; t.IIc = tc.z;
+                    float scA = st.sc[2 * lane][pos];
+                    if (kCorner && (c <= caA || c >= cbA)) scA = -9.0f;
+                    S5 nA;
+                    int code = 0;
+                    if (kCodes) {
+                        code = dp_cell(dg, u, lA, qa, t, scA, nA);
+                        if (bstA < nA.MM) { bstA = nA.MM; bcA = c; }
+                    } else {
+                        dp_states(dg, u, lA, qa, t, scA, nA);
+                        bstA = fmaxf(bstA, nA.MM);
+                    }
+                    if (doB) {
+                        float scB = st.sc[2 * lane + 1][pos];
+                        if (kCorner && (c <= caB || c >= cbB)) scB = -9.0f;
+                        // diagonal of (rB, c) = (rA, c-1): row A's left state; a
+                        // 32-row band's last row takes zeros at column 0
+                        S5 dB = lA;
+                        if (kChecked && lastB && c == 0) dB = S5{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                        S5 nB;
+                        if (kCodes) {
+                            code |= dp_cell(dB, nA, lB, qb, t, scB, nB) << 4;
+                            if (bstB < nB.MM) { bstB = nB.MM; bcB = c; }
+                        } else {
+                            dp_states(dB, nA, lB, qb, t, scB, nB);
+                            bstB = fmaxf(bstB, nB.MM);
+                        }
+                        lB = nB;
+                        if (lane == 31) {
+                            st.soa[pos] = make_float4(nB.MM, nB.MI, nB.IM, nB.DN);
+                            st.sob[pos] = nB.ND;
+                        }
+                    }
+                    if (kCodes) st.bt[lane][pos] = (uint8_t)code;
+                    lA = nA;
+                }
+                dg = u;
+            };
+
+            __syncwarp();   // the previous band's tiles are no longer read
+            issue(0);
+            int hflushed = 0;   // pieces 0 .. hflushed-1 are written back
+            // steps with every lane inside the profile and on a row (the
+            // unchecked steps): [32, Ld) on a full band
+            const int fast0 = full ? 32 : nsteps, fast1 = full ? Ld : nsteps;
+            for (int H = 0;; H++) {
+                const int sb = (H == 0) ? 0 : kPiece * H - off;   // lane 0 enters piece H
+                if (sb >= nsteps) break;
+                const int se = min(kPiece * H + kPiece - off, nsteps);
+                __syncwarp();
+                // lane 31 left piece H-3 two steps ago; its ring slot takes piece H+1
+                if (H >= 3 && H - 3 <= h_last) { flush(H - 3); hflushed = H - 2; }
+                if (H <= h_last) {
+                    const bool more = H + 1 <= h_last;
+                    if (more) issue(H + 1);
+                    else cp_async_commit();   // an empty group keeps the wait accounting
+                    if (!await(H, more)) { ok = false; break; }
+                }
+                const int f0 = max(sb, fast0), f1 = min(se, fast1);
+                if (f0 < f1) {
+                    for (int s = sb; s < f0; s++) step(s, kTrue(), kTrue());
+                    if (bcorner) {
+#pragma unroll 2
+                        for (int s = f0; s < f1; s++) step(s, kFalse(), kTrue());
+                    } else {
+#pragma unroll 2
+                        for (int s = f0; s < f1; s++) step(s, kFalse(), kFalse());
+                    }
+                    for (int s = f1; s < se; s++) step(s, kTrue(), kTrue());
+                } else {
+                    for (int s = sb; s < se; s++) step(s, kTrue(), kTrue());
+                }
+            }
+            if (!ok) break;
+            __syncwarp();
+            for (int h = hflushed; h <= h_last; h++) flush(h);
+            // the band's maxima into the lane's, in row-major order
+            if (kCodes) {
+                if (best < bstA) { best = bstA; bestr = rA; bestc = bcA; }
+                if (best < bstB) { best = bstB; bestr = rB; bestc = bcB; }
             } else {
-                for (int s = sb; s < se; s++) step(s, kTrue(), kTrue());
+                best = fmaxf(best, fmaxf(bstA, bstB));
             }
         }
-        if (!ok) break;
-        __syncwarp();
-        for (int h = hflushed; h <= h_last; h++) flush(h);
-        // the band's maxima into the lane's, in row-major order
-        if (best < bstA) { best = bstA; bestr = rA; bestc = bcA; }
-        if (best < bstB) { best = bstB; bestr = rB; bestc = bcB; }
+    };
+
+    // The codes are read only by the backtrace of a profile whose maximum
+    // exceeds the threshold (the finalization skips the others), so a
+    // sweep without them finds the maximum first and a candidate sweeps
+    // again with them; code_thld = -inf: one sweep with codes for all.
+    bool codes = true;
+    if (a.code_thld != -INFINITY) {
+        sweep(kFalse());
+        for (int o = 16; o >= 1; o >>= 1) best = fmaxf(best, __shfl_xor_sync(kFull, best, o));
+        codes = ok && best > a.code_thld;
     }
+    if (codes) sweep(kTrue());
     if (!ok) {
         // a staging wait gave up (its copies drained): flag the profile and
         // the launch, and return
@@ -496,6 +545,14 @@ dp1_kernel(const Dp1Args a)
             a.maxsc[pl] = __int_as_float(0x7fc00000);
             a.maxcoords[pl] = 0xffffffffu;
             if (a.err) atomicExch(a.err, 1);
+        }
+        return;
+    }
+    if (!codes) {
+        // no candidate: the maximum alone (the coordinates are not read)
+        if (lane == 0) {
+            a.maxsc[pl] = best;
+            a.maxcoords[pl] = 0u;
         }
         return;
     }

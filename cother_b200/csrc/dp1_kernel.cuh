@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <math.h>
 #include "layout.h"
 
 namespace cbp {
@@ -33,6 +34,10 @@ struct Dp1Args {
     Dp1Rec* recs = nullptr;          // [nprof]
     int warps = 2;                   // warps (profiles) per block of dp1_kernel: 1 or 2
     int* err = nullptr;              // set to 1 when a staging wait gave up (may be null)
+    // backtrack codes are computed for the profiles whose maximum exceeds
+    // code_thld (the finalization's threshold: it backtraces only those);
+    // -inf: for every profile
+    float code_thld = -INFINITY;
 };
 
 void launch_dp1(const Dp1Args& a, cudaStream_t stream);

@@ -82,12 +82,19 @@ typedef struct cbp_options {
                        * column-ordering window, phase-1 DP warps per block) on a
                        * sample of the slab and keep the fastest (no counterpart in
                        * the reference). Results do not depend on the choice. */
+    int   all_codes;  /* 1: the phase-1 DP writes backtrack codes for every database
+                       * profile (what cbp_read_btck shows then matches the
+                       * reference's matrix everywhere); 0: only for the profiles
+                       * whose DP maximum exceeds the score threshold, the only
+                       * ones the finalization backtraces -- the others take one
+                       * sweep without codes. Results do not depend on it. */
 } cbp_options;
 
 /* Fill *opt with the values of the parity configuration:
  * SSSWGT=0.12, CVSWGT=0, DDMSWGT=0.2, DSTSEGM=6, MAPALN=1, MINPP=0.28,
  * SSEMODEL=2, X_UNINF=1, EVAL=10, NOHITS=NOALNS=700; the plain FP32
- * profile-profile form and the kernel tuner on. */
+ * profile-profile form, the kernel tuner on and backtrack codes for the
+ * finalization's candidates only. */
 void cbp_default_options(cbp_options* opt);
 
 /* Create a context on `device`.

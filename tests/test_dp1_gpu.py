@@ -6,9 +6,11 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _search(q, db, ss, thld, max_slab=0):
+def _search(q, db, ss, thld, max_slab=0, all_codes=1):
     import cother_b200 as cb
-    bp = cb.BatchProcessing(ss)
+    o = cb.Options.defaults()
+    o.all_codes = all_codes
+    bp = cb.BatchProcessing(ss, o)
     if max_slab:
         bp.set_max_slab_positions(max_slab)
     bp.set_score_threshold(thld)
@@ -17,7 +19,7 @@ def _search(q, db, ss, thld, max_slab=0):
     return bp
 
 
-def _compare(bp, oracle_lib, q, db, thld, p0=0):
+def _compare(bp, oracle_lib, q, db, thld, p0=0, all_codes=True, mixed=True):
     sc, ms, first = bp.read_score_matrix(q.npositions, db.npositions)
     assert first == p0
     rec, plist = bp.read_phase1()
@@ -25,7 +27,17 @@ def _compare(bp, oracle_lib, q, db, thld, p0=0):
     col0 = int(db.starts[p0])
     btck = bp.read_btck(q.npositions, sc.shape[1])
     orec, obt = oracle_lib.dp1(q, db, sc, col0, p0, nprof, thld)
-    assert np.array_equal(btck, obt)
+    if all_codes:
+        assert np.array_equal(btck, obt)
+    else:
+        # codes only for the finalization's candidates: DP maximum > threshold
+        cand = orec["maxsc"] > np.float32(thld)
+        if mixed:
+            assert cand.any() and not cand.all()
+        for k in np.nonzero(cand)[0]:
+            c0 = int(db.starts[p0 + k]) - col0
+            L = int(db.lens[p0 + k])
+            assert np.array_equal(btck[:, c0:c0 + L], obt[:, c0:c0 + L]), k
     assert np.array_equal(rec["passed"], orec["passed"])
     assert np.array_equal(rec["score"], orec["score"])
     m = orec["passed"] == 1
@@ -43,6 +55,27 @@ def test_dp1_workload_with_homologs(oracle_lib, ss_table):
     bp = _search(q, db, ss_table, thld)
     rec, plist = _compare(bp, oracle_lib, q, db, thld)
     assert len(plist) >= 8
+    bp.close()
+
+
+def test_dp1_codes_for_candidates_only(oracle_lib, ss_table):
+    """The default: a sweep without codes finds each profile's maximum and
+    only the profiles above the threshold sweep again with codes; records,
+    pass list and the candidates' codes equal the oracle's."""
+    from cother_b200 import synth
+    q, db = synth.make_workload("q200_db1k", seed=5, ndb=48, homologs=0.25)
+    thld, _ = oracle_lib.score_threshold(q.npositions, 180 * 1000)
+    bp = _search(q, db, ss_table, thld, all_codes=0)
+    rec, plist = _compare(bp, oracle_lib, q, db, thld, all_codes=False)
+    assert len(plist) >= 8
+    bp.close()
+    bp = _search(q, db, ss_table, thld, max_slab=2000, all_codes=0)
+    lens, p0, acc = db.lens, 0, 0
+    for p, L in enumerate(lens):
+        if acc + L > 2000:
+            p0, acc = p, 0
+        acc += int(L)
+    _compare(bp, oracle_lib, q, db, thld, p0=p0, all_codes=False, mixed=False)
     bp.close()
 
 

@@ -15,6 +15,7 @@ def _run(q, db, ss, variant=None, autotune=1):
     import cother_b200 as cb
     o = cb.Options.defaults()
     o.autotune = autotune
+    o.all_codes = 1     # compare the whole backtrack matrix
     with cb.BatchProcessing(ss, o) as bp:
         if variant is not None:
             bp.set_kernels(q.npositions, *variant)

@@ -21,7 +21,9 @@ pytestmark = pytest.mark.gpu
 
 def _regular_path(q, db, ss, thld):
     import cother_b200 as cb
-    bp = cb.BatchProcessing(ss)
+    o = cb.Options.defaults()
+    o.all_codes = 1     # backtrack codes of every profile, whatever passes
+    bp = cb.BatchProcessing(ss, o)
     bp.set_score_threshold(thld)
     bp.transfer_cpm_data(db)
     bp.process_score_matrix(q)
