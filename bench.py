@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tc-forms", action="store_true",
+                    help="skip the tensor-core forms measured after the timed run")
     ap.add_argument("--tc", default="plain", choices=["plain", "bf16", "tf32"],
                     help="form of the profile-profile term: FP32 CUDA cores or tensor cores "
                          "(BF16x3 / TF32x3 hi-lo split)")
@@ -234,6 +236,36 @@ def cpu_baseline(q, db, ss, seconds: float, db_len: int, nseqs: int, cvswgt: flo
     timer = CpuTimer(q, db, ss, db_len, nseqs, cvswgt)
     out = timer.measure(seconds * 0.6, ncpu)
     out["single_thread"] = timer.measure(seconds * 0.4, 1)
+    return out
+
+
+def tc_forms(cb, ss, plain_opts, q, db, db_len: int, nseqs: int, plain_digest: str) -> dict:
+    """The tensor-core forms (BF16x3, TF32x3) of the whole path on the same
+    query and database: GCUPS from the stages' device time over two steps
+    after one warm-up, the score stage's time, and whether the top-50 hit
+    list equals the plain form's."""
+    out = {}
+    for name, form in (("bf16x3", cb.TC_BF16X3), ("tf32x3", cb.TC_TF32X3)):
+        o = cb.Options.defaults()
+        for f, _ in cb.Options._fields_:
+            setattr(o, f, getattr(plain_opts, f))
+        o.tc_form = form
+        with cb.BatchProcessing(ss, o) as bp:
+            bp.transfer_cpm_data(db)
+            bp.set_db_details(db_len, nseqs)
+            bp.set_query_len(q.npositions)
+            bp.process_score_matrix(q)
+            ms, score_ms = 0.0, 0.0
+            for _ in range(2):
+                bp.process_score_matrix(q)
+                st = bp.stage_times()
+                ms += sum(st)
+                score_ms += st[0]
+            recs, order = bp.hit_records(), bp.hit_list()
+            digest = hashlib.sha1(recs[order[:50], 1].view(np.uint32).tobytes()).hexdigest()[:16]
+        out[name] = {"value": float(q.npositions) * db.npositions * 2 / (ms / 1e3) / 1e9, "unit": "GCUPS",
+                     "score_matrix_ms": score_ms / 2, "top50_digest": digest,
+                     "top50_same_as_plain": digest == plain_digest}
     return out
 
 
@@ -497,8 +529,12 @@ def main():
                 "tuning": bp.tuning(Lq), "roofline": roof, "clocks": clocks}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds, db_len, nseqs, args.cvswgt)
-        print(json.dumps(line))
     bp.close()
+    if rank == 0:
+        if world == 1 and args.tc == "plain" and not args.no_tc_forms:
+            # the precision forms on the same workload, after the timed run
+            line["tc_forms"] = tc_forms(cb, ss, opts, q, db, db_len, nseqs, line["top50_digest"])
+        print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
 

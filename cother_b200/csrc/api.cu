@@ -582,11 +582,15 @@ void tune_kernels(cbp_context* c, const ScoreArgs& base, int p0, int p1, Tuning&
     d.maxsc = c->dpmax.as<float>();
     d.maxcoords = c->dpcoords.as<uint32_t>();
     d.recs = c->dprecs.as<Dp1Rec>();
+    // timed as the search runs it: the launch without backtrack codes over
+    // every profile, then the codes launch, here with no candidate
+    d.code_thld = INFINITY;
     int bd = 0;
     for (int k = 0; k < kDpCandidates; k++) {
         d.warps = kDpWarpsCand[k];
-        t.dp_ms[k] = time_it([&] { launch_dp1(d, c->stream); });
-        c->launches += 2;
+        int nl = 0;
+        t.dp_ms[k] = time_it([&] { nl = launch_dp1(d, c->stream); });
+        c->launches += 2 * (uint64_t)nl;   // two timed repetitions
         if (t.dp_ms[k] < t.dp_ms[bd]) bd = k;
     }
     t.rows = kScoreRowsCand[bs];
@@ -843,6 +847,7 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
         // each query's DP, finalization and pass list; with the plain form
         // one CUDA graph, captured here and swapped into the context's
         // executable graph by an update of its parameters
+        int dp_launches = 0;
         auto phase1 = [&](bool capturing) {
             auto mark = [&](cudaEvent_t e) {
                 if (capturing) CBP_CUDA(cudaEventRecordWithFlags(e, c->stream, cudaEventRecordExternal));
@@ -855,7 +860,8 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
             launch_score_matrix(a, c->stream);
             mark(c->ev[1]);
             CBP_CUDA(cudaMemsetAsync(c->dp1err.p, 0, sizeof(int), c->stream));
-            for (size_t k = 0; k < nq; k++) launch_dp1(d[k], c->stream);
+            dp_launches = 0;
+            for (size_t k = 0; k < nq; k++) dp_launches += launch_dp1(d[k], c->stream);
             mark(c->ev[2]);
             for (size_t k = 0; k < nq; k++) {
                 launch_dp1_finalize(d[k], res[k].score_thld, c->stream);
@@ -896,9 +902,9 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
             CBP_CUDA(cudaGraphLaunch(c->phase1_exec, c->stream));
             c->graph_launches += 1;
         }
-        c->launches += 2 + 3 * (uint64_t)nq;
+        c->launches += 2 + (uint64_t)dp_launches + 2 * (uint64_t)nq;
         c->stage_launches[0] += 2;
-        c->stage_launches[1] += nq;
+        c->stage_launches[1] += (uint64_t)dp_launches;
         c->stage_launches[2] += 2 * (uint64_t)nq;
         std::vector<int> npass(nq, 0);
         for (size_t k = 0; k < nq; k++)

@@ -67,12 +67,18 @@ __device__ __forceinline__ int corner_edge(int Lq, int Ld)
 // A lane's two backtrack codes share one byte of a shared tile; the band's
 // bottom row goes to a shared ring too. Both are written back once lane 31
 // has left a piece: four code bytes per store, the strip coalesced.
+//
+// Occupancy. The kernel is bound by the latency of each warp's chain of
+// dependent steps, so the SM's throughput grows with the warps resident.
+// The launch that finds the maxima has no backtrack tile and needs about
+// 100 registers instead of about 150, so more of its warps share an SM.
 constexpr int kBand = 64;              // query rows per band (two per lane)
 constexpr int kRing = 64;              // staged columns
 constexpr int kPiece = 16;             // columns per staged piece
 constexpr int kSlots = kRing / kPiece; // ring slots
 constexpr unsigned long long kWaitNs = 1000000000ull;   // a staging wait gives up after 1 s
 
+template <bool kCodes>
 struct alignas(128) DpStage {
     float sc[kBand][kRing];            // scores of the band's rows
     float4 tra[kRing];                 // transitions of the column: MM, IM, DM, MD
@@ -81,7 +87,7 @@ struct alignas(128) DpStage {
     float spb[kRing];                  // ... and ND
     float4 soa[kRing];                 // this band's bottom row, for the next band
     float sob[kRing];
-    uint8_t bt[32][kRing];             // codes of rows A (low nibble) and B (high nibble)
+    uint8_t bt[kCodes ? 32 : 1][kRing]; // codes of rows A (low nibble) and B (high nibble)
     unsigned long long bar[kSlots];    // completion of each slot's score rows
 };
 
@@ -203,7 +209,7 @@ __device__ __forceinline__ Q7 query_trn(const float* __restrict__ qtrn, long lon
 // shared memory. kBulk: score rows by bulk copies (the slab width is a
 // multiple of 4 floats and the buffers are aligned); otherwise by 4-byte
 // cp.async with the ring unshifted.
-template <int kWarps, bool kBulk>
+template <int kWarps, bool kBulk, bool kCodes>
 __global__ void __launch_bounds__(32 * kWarps)
 dp1_kernel(const Dp1Args a)
 {
@@ -211,7 +217,7 @@ dp1_kernel(const Dp1Args a)
     const int lane = threadIdx.x & 31;
     const int pl = blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (pl >= a.nprof) return;  // whole warp
-    DpStage& st = reinterpret_cast<DpStage*>(s_dyn)[threadIdx.x >> 5];
+    DpStage<kCodes>& st = reinterpret_cast<DpStage<kCodes>*>(s_dyn)[threadIdx.x >> 5];
     const int p = a.p0 + pl;
     const int Ld = a.db.plen[p];
     const long long colb = a.db.pstart[p] - a.col0;
@@ -256,7 +262,7 @@ dp1_kernel(const Dp1Args a)
     // One sweep over the profile's DP. kCodes: with the backtrack codes and
     // the coordinates of the maximum; without them, the maximum alone.
     auto sweep = [&](auto codes_tag) {
-        constexpr bool kCodes = decltype(codes_tag)::value;
+        constexpr bool kSweepCodes = decltype(codes_tag)::value;
         best = 0.0f;
         bestr = 0;
         bestc = 0;
@@ -384,7 +390,7 @@ dp1_kernel(const Dp1Args a)
                 const uint32_t pw[4] = {pk.x, pk.y, pk.z, pk.w};
 #pragma unroll
                 for (int k = 0; k < 2; k++) {
-                    if (!kCodes || r0 + 2 * lane + k >= Lq) continue;
+                    if (!kSweepCodes || r0 + 2 * lane + k >= Lq) continue;
                     uint8_t* dst = B + (long long)(r0 + 2 * lane + k) * ld + c0;
 #pragma unroll
                     for (int wd = 0; wd < 4; wd++) {
@@ -446,7 +452,7 @@ dp1_kernel(const Dp1Args a)
                     if (kCorner && (c <= caA || c >= cbA)) scA = -9.0f;
                     S5 nA;
                     int code = 0;
-                    if (kCodes) {
+                    if (kSweepCodes) {
                         code = dp_cell(dg, u, lA, qa, t, scA, nA);
                         if (bstA < nA.MM) { bstA = nA.MM; bcA = c; }
                     } else {
@@ -461,7 +467,7 @@ dp1_kernel(const Dp1Args a)
                         S5 dB = lA;
                         if (kChecked && lastB && c == 0) dB = S5{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
                         S5 nB;
-                        if (kCodes) {
+                        if (kSweepCodes) {
                             code |= dp_cell(dB, nA, lB, qb, t, scB, nB) << 4;
                             if (bstB < nB.MM) { bstB = nB.MM; bcB = c; }
                         } else {
@@ -474,7 +480,7 @@ dp1_kernel(const Dp1Args a)
                             st.sob[pos] = nB.ND;
                         }
                     }
-                    if (kCodes) st.bt[lane][pos] = (uint8_t)code;
+                    if (kSweepCodes) st.bt[lane][pos] = (uint8_t)code;
                     lA = nA;
                 }
                 dg = u;
@@ -518,7 +524,7 @@ dp1_kernel(const Dp1Args a)
             __syncwarp();
             for (int h = hflushed; h <= h_last; h++) flush(h);
             // the band's maxima into the lane's, in row-major order
-            if (kCodes) {
+            if (kSweepCodes) {
                 if (best < bstA) { best = bstA; bestr = rA; bestc = bcA; }
                 if (best < bstB) { best = bstB; bestr = rB; bestc = bcB; }
             } else {
@@ -528,31 +534,28 @@ dp1_kernel(const Dp1Args a)
     };
 
     // The codes are read only by the backtrace of a profile whose maximum
-    // exceeds the threshold (the finalization skips the others), so a
-    // sweep without them finds the maximum first and a candidate sweeps
-    // again with them; code_thld = -inf: one sweep with codes for all.
-    bool codes = true;
-    if (a.code_thld != -INFINITY) {
+    // exceeds the threshold (the finalization skips the others). So a first
+    // launch without them (kCodes false, a smaller stage) finds every
+    // profile's maximum, and a second launch sweeps the candidates again
+    // with them; code_thld = -inf: the second launch alone, for all.
+    if (!kCodes) {
         sweep(kFalse());
         for (int o = 16; o >= 1; o >>= 1) best = fmaxf(best, __shfl_xor_sync(kFull, best, o));
-        codes = ok && best > a.code_thld;
+        if (lane == 0) {
+            // a staging wait that gave up flags the profile and the launch
+            a.maxsc[pl] = ok ? best : __int_as_float(0x7fc00000);
+            a.maxcoords[pl] = ok ? 0u : 0xffffffffu;
+            if (!ok && a.err) atomicExch(a.err, 1);
+        }
+        return;
     }
-    if (codes) sweep(kTrue());
+    if (a.code_thld != -INFINITY && !(a.maxsc[pl] > a.code_thld)) return;   // not a candidate
+    sweep(kTrue());
     if (!ok) {
-        // a staging wait gave up (its copies drained): flag the profile and
-        // the launch, and return
         if (lane == 0) {
             a.maxsc[pl] = __int_as_float(0x7fc00000);
             a.maxcoords[pl] = 0xffffffffu;
             if (a.err) atomicExch(a.err, 1);
-        }
-        return;
-    }
-    if (!codes) {
-        // no candidate: the maximum alone (the coordinates are not read)
-        if (lane == 0) {
-            a.maxsc[pl] = best;
-            a.maxcoords[pl] = 0u;
         }
         return;
     }
@@ -595,7 +598,7 @@ dp1_finalize_kernel(const Dp1Args a, float thld)
     rec.beg = 0;
     rec.end = 0;
     rec.passed = 0;
-    if (maxsc <= thld) {
+    if (!(maxsc > thld)) {   // a NaN maximum (a flagged profile) never passes
         if (lane == 0) a.recs[pl] = rec;
         return;
     }
@@ -696,34 +699,47 @@ pass_compact_kernel(const Dp1Args a, int* __restrict__ pass_idx, long long* __re
 
 }  // namespace
 
-template <int kW, bool kBulk>
+template <int kW, bool kBulk, bool kCodes>
 void launch_dp1_variant(const Dp1Args& a, cudaStream_t stream)
 {
-    const size_t smem = (size_t)kW * sizeof(DpStage);
-    dp1_kernel<kW, kBulk><<<(unsigned)ceil_div(a.nprof, kW), 32 * kW, smem, stream>>>(a);
+    const size_t smem = (size_t)kW * sizeof(DpStage<kCodes>);
+    dp1_kernel<kW, kBulk, kCodes><<<(unsigned)ceil_div(a.nprof, kW), 32 * kW, smem, stream>>>(a);
     CBP_CHECK_LAUNCH();
 }
 
 void dp1_set_attributes()
 {
     // dynamic shared memory above 48 KB (two warps per block) needs an opt-in
-    CBP_CUDA(cudaFuncSetAttribute(dp1_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(2 * sizeof(DpStage))));
-    CBP_CUDA(cudaFuncSetAttribute(dp1_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(2 * sizeof(DpStage))));
+    CBP_CUDA(cudaFuncSetAttribute(dp1_kernel<2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * sizeof(DpStage<true>))));
+    CBP_CUDA(cudaFuncSetAttribute(dp1_kernel<2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * sizeof(DpStage<true>))));
+    CBP_CUDA(cudaFuncSetAttribute(dp1_kernel<2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * sizeof(DpStage<false>))));
+    CBP_CUDA(cudaFuncSetAttribute(dp1_kernel<2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * sizeof(DpStage<false>))));
 }
 
-void launch_dp1(const Dp1Args& a, cudaStream_t stream)
+template <bool kCodes>
+void launch_dp1_pass(const Dp1Args& a, bool bulk, cudaStream_t stream)
 {
-    if (a.nprof <= 0) return;
+    switch (a.warps) {
+    case 1: bulk ? launch_dp1_variant<1, true, kCodes>(a, stream) : launch_dp1_variant<1, false, kCodes>(a, stream); break;
+    case 2: bulk ? launch_dp1_variant<2, true, kCodes>(a, stream) : launch_dp1_variant<2, false, kCodes>(a, stream); break;
+    default: throw Error(CBP_ERR_ARG, "phase-1 DP warps per block must be 1 or 2");
+    }
+}
+
+int launch_dp1(const Dp1Args& a, cudaStream_t stream)
+{
+    if (a.nprof <= 0) return 0;
     // bulk copies of score rows need 16-byte aligned rows and 4-byte
     // aligned backtrack words
     const bool bulk = (a.ld % 4 == 0) && ((uintptr_t)a.scores % 16 == 0) && ((uintptr_t)a.btck % 4 == 0);
-    switch (a.warps) {
-    case 1: bulk ? launch_dp1_variant<1, true>(a, stream) : launch_dp1_variant<1, false>(a, stream); break;
-    case 2: bulk ? launch_dp1_variant<2, true>(a, stream) : launch_dp1_variant<2, false>(a, stream); break;
-    default: throw Error(CBP_ERR_ARG, "phase-1 DP warps per block must be 1 or 2");
-    }
+    const bool split = a.code_thld != -INFINITY;
+    if (split) launch_dp1_pass<false>(a, bulk, stream);
+    launch_dp1_pass<true>(a, bulk, stream);
+    return split ? 2 : 1;
 }
 
 void launch_dp1_finalize(const Dp1Args& a, float thld, cudaStream_t stream)

@@ -40,7 +40,11 @@ struct Dp1Args {
     float code_thld = -INFINITY;
 };
 
-void launch_dp1(const Dp1Args& a, cudaStream_t stream);
+// Phase-1 DP of the slab's profiles; returns the number of kernel launches:
+// with a finite code_thld a launch without backtrack codes finds every
+// profile's maximum and a second one sweeps the candidates again with codes
+// (2), with code_thld = -inf the second alone, for all profiles (1).
+int launch_dp1(const Dp1Args& a, cudaStream_t stream);
 // Per device, before the first launch_dp1 with two warps per block (and
 // outside any stream capture): the shared-memory opt-in of the DP kernels.
 void dp1_set_attributes();
