@@ -181,6 +181,8 @@ constexpr int kDpCandidates = 2;
 constexpr int kScoreRowsCand[kScoreCandidates] = {16, 8, 32, 16, 16};
 constexpr int kWindowCand[kScoreCandidates] = {1024, 1024, 1024, 256, 4096};
 constexpr int kDpWarpsCand[kDpCandidates] = {2, 1};
+constexpr int kPreferredScoreCand = 2;     // 32 rows, window 1,024
+constexpr float kTuneMargin = 0.015f;      // a candidate must be this much faster to replace it
 struct Tuning {
     int rows = 16, window = kOrderWindow, dp_warps = 2;
     bool tuned = false;
@@ -568,6 +570,11 @@ void tune_kernels(cbp_context* c, const ScoreArgs& base, int p0, int p1, Tuning&
         c->launches += 4;
         if (t.score_ms[k] < t.score_ms[bs]) bs = k;
     }
+    // The candidates' sample times lie within about 1 % of each other, the
+    // sample's noise. Unless one is clearly faster, keep 32 rows per block
+    // with the default window: the fewest re-reads of the database lists,
+    // and the fastest on full-size slabs.
+    if (t.score_ms[bs] > (1.0f - kTuneMargin) * t.score_ms[kPreferredScoreCand]) bs = kPreferredScoreCand;
     Dp1Args d;
     d.scores = a.scores;
     d.ld = a.ld;
