@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tc-forms", action="store_true",
                     help="skip the tensor-core forms measured after the timed run")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="skip the short serving run after the timed run")
     ap.add_argument("--tc", default="plain", choices=["plain", "bf16", "tf32"],
                     help="form of the profile-profile term: FP32 CUDA cores or tensor cores "
                          "(BF16x3 / TF32x3 hi-lo split)")
@@ -338,31 +340,23 @@ def run_reference(args):
     print(json.dumps(line))
 
 
-def run_serve(args):
-    """--serve: Poisson arrivals of request queries against a resident
-    database, served by the library's C++ request loop (concurrent slots,
-    continuous batching of the waiting queries into one pass over the
-    database); reports completed queries per second and the latency
-    (arrival to results) for each offered load in --rate (comma list)."""
+def serve_loads(db, ss, opts, rates, nqueries: int, slots: int, max_batch: int, seed: int):
+    """Poisson arrivals of `nqueries` request queries per offered load in
+    `rates` (queries/s) against the resident database `db`, served by the
+    library's C++ request loop; one summary dict per load, and the loop's
+    memory budget."""
     from cother_b200 import synth
     from cother_b200.serving import SearchServer, latency_summary
-    import cother_b200 as cb
-    workload = args.workload if args.workload != DEFAULT_WORKLOAD else "serve_db100k"
-    ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
-    _, db = synth.make_workload(workload, seed=args.seed, ndb=args.ndb)
-    rates = [float(x) for x in str(args.rate).split(",")]
-    opts = cb.Options.defaults()
-    opts.tc_form = {"plain": cb.TC_PLAIN, "bf16": cb.TC_BF16X3, "tf32": cb.TC_TF32X3}[args.tc]
     loads = []
-    with SearchServer(db, ss, opts, slots=args.slots, max_batch=args.max_batch) as srv:
-        srv.submit(synth.serving_queries(1, seed=args.seed + 99)[0]).result()   # warm-up, not timed
+    with SearchServer(db, ss, opts, slots=slots, max_batch=max_batch) as srv:
+        srv.submit(synth.serving_queries(1, seed=seed + 99)[0]).result()   # warm-up, not timed
         for li, rate in enumerate(rates):
-            queries = synth.serving_queries(args.queries, seed=args.seed + li)
-            rng = np.random.default_rng(args.seed + li)
-            gaps = rng.exponential(1.0 / rate, args.queries)
+            queries = synth.serving_queries(nqueries, seed=seed + li)
+            rng = np.random.default_rng(seed + li)
+            gaps = rng.exponential(1.0 / rate, nqueries)
             t0 = time.perf_counter()
             futs = []
-            for k in range(args.queries):
+            for k in range(nqueries):
                 t0 += gaps[k]
                 delay = t0 - time.perf_counter()
                 if delay > 0:
@@ -372,11 +366,29 @@ def run_serve(args):
             s = latency_summary(res)
             cells = sum(q.npositions for q in queries) * db.npositions
             wall = max(r["finish"] for r in res) - min(r["arrival"] for r in res)
-            loads.append({"offered_qps": rate, "queries": args.queries, "queries_per_s": s["queries_per_s"],
+            loads.append({"offered_qps": rate, "queries": nqueries, "queries_per_s": s["queries_per_s"],
                           "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"], "service_p50_ms": s["service_p50_ms"],
                           "mean_batch": s["mean_batch"], "gcups": cells / wall / 1e9,
                           "query_lens": [q.npositions for q in queries]})
         budget = srv.budget
+    return loads, budget
+
+
+def run_serve(args):
+    """--serve: Poisson arrivals of request queries against a resident
+    database, served by the library's C++ request loop (concurrent slots,
+    continuous batching of the waiting queries into one pass over the
+    database); reports completed queries per second and the latency
+    (arrival to results) for each offered load in --rate (comma list)."""
+    from cother_b200 import synth
+    import cother_b200 as cb
+    workload = args.workload if args.workload != DEFAULT_WORKLOAD else "serve_db100k"
+    ss = np.load(os.path.join(ROOT, "tests", "golden", "ssss.npy"))
+    _, db = synth.make_workload(workload, seed=args.seed, ndb=args.ndb)
+    rates = [float(x) for x in str(args.rate).split(",")]
+    opts = cb.Options.defaults()
+    opts.tc_form = {"plain": cb.TC_PLAIN, "bf16": cb.TC_BF16X3, "tf32": cb.TC_TF32X3}[args.tc]
+    loads, budget = serve_loads(db, ss, opts, rates, args.queries, args.slots, args.max_batch, args.seed)
     best = max(loads, key=lambda x: x["queries_per_s"])
     print(json.dumps({
         "metric": "queries_per_s", "value": best["queries_per_s"], "unit": "queries/s",
@@ -385,6 +397,23 @@ def run_serve(args):
         "config": {"workload": workload, "db_profiles": db.nprofiles, "db_positions": db.npositions,
                    "slots": args.slots, "max_batch": args.max_batch, "tc_form": args.tc,
                    "memory_budget_bytes": budget}}))
+
+
+def serving_summary(cb, ss, seed: int) -> dict:
+    """A short run of the serving configuration after the timed steps: the
+    resident 100,000-profile database, six Poisson requests at 20 queries/s,
+    3 slots, batches of up to 4, the BF16x3 tensor-core score path."""
+    from cother_b200 import synth
+    _, db = synth.make_workload("serve_db100k", seed=seed)
+    opts = cb.Options.defaults()
+    opts.tc_form = cb.TC_BF16X3
+    loads, budget = serve_loads(db, ss, opts, [20.0], 6, 3, 4, seed)
+    out = dict(loads[0])
+    out.update({"workload": "serve_db100k", "db_profiles": db.nprofiles, "db_positions": db.npositions,
+                "slots": 3, "max_batch": 4, "tc_form": "bf16", "memory_budget_bytes": budget,
+                "note": "shortened stream (6 requests); the configuration's 2,000 would take hours at "
+                        "this capacity"})
+    return out
 
 
 def main():
@@ -534,6 +563,9 @@ def main():
         if world == 1 and args.tc == "plain" and not args.no_tc_forms:
             # the precision forms on the same workload, after the timed run
             line["tc_forms"] = tc_forms(cb, ss, opts, q, db, db_len, nseqs, line["top50_digest"])
+        if world == 1 and not args.no_serving and args.ndb is None and args.workload == DEFAULT_WORKLOAD:
+            del q, db
+            line["serving"] = serving_summary(cb, ss, args.seed)
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

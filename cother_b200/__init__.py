@@ -98,6 +98,7 @@ def load_library(path: str | None = None):
                                   ctypes.POINTER(sz)]),
         "cbp_read_btck": (i32, [vp, vp, sz]),
         "cbp_read_slab_columns": (i32, [vp, sz, sz, vp, vp, vp, sz]),
+        "cbp_read_map_fb": (i32, [vp, sz, vp, sz, ctypes.POINTER(sz)]),
         "cbp_read_fits": (i32, [vp, vp, sz, ctypes.POINTER(sz)]),
         "cbp_score_threshold": (None, [sz, ctypes.c_uint64, f32, f32, f32, ctypes.POINTER(f32),
                                        ctypes.POINTER(f32)]),
@@ -450,6 +451,17 @@ class BatchProcessing:
         _check(load_library().cbp_read_slab_columns(self._h, int(first_col), int(ncols), sc.ctypes.data,
                                                      ms.ctypes.data, bt.ctypes.data, sc.shape[1]))
         return sc[:, :ncols], ms[:, :ncols], bt[:, :ncols]
+
+    def map_fb(self, pair: int, nrows: int) -> np.ndarray:
+        """The MAP stage's forward + backward log match-state values of pair
+        `pair` of the last slab's pass list, [nrows][profile length]
+        (cbp_read_map_fb)."""
+        L = load_library()
+        n = ctypes.c_size_t()
+        _check(L.cbp_read_map_fb(self._h, int(pair), None, 0, ctypes.byref(n)))
+        fb = np.zeros((nrows, max(1, n.value)), np.float32)
+        _check(L.cbp_read_map_fb(self._h, int(pair), fb.ctypes.data, fb.shape[1], ctypes.byref(n)))
+        return fb[:, :n.value]
 
     def format_hits(self, descs=None, options=None):
         """Per-hit text of the last search in the finalizer's order: a list

@@ -247,6 +247,14 @@ struct cbp_context {
     DevBuf qtrn;               // batches: each query's transitions as [7][Lq+1]
 
     int h_maperr = 0;   // set by the MAP stage when a wait between warps gave up
+    // the last MAP realignment (last slab, last query of the call), for
+    // cbp_read_map_fb: its pass list, phase-2 columns and band geometry
+    int last_map_np = 0;
+    long long last_map_nd = 0;
+    int last_map_Lq = 0;
+    int last_map_p0 = 0;
+    const int* last_map_pass_idx = nullptr;
+    const long long* last_map_pass_dst = nullptr;
     int h_dp1err = 0;   // set by the phase-1 DP when a staging wait gave up
     bool score_thld_set = false, logE_thld_set = false;
     // results of the last process() call, all slabs
@@ -714,6 +722,7 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
         }
     }
     c->launches = 0;
+    c->last_map_np = 0;
     for (float& m : c->stage_ms) m = 0.f;
     for (uint64_t& m : c->stage_launches) m = 0;
     c->res.clear();
@@ -1035,6 +1044,12 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
                 CBP_CUDA(cudaEventRecord(c->ev[6], c->stream));
                 launch_map(mp, c->stream);
                 CBP_CUDA(cudaEventRecord(c->ev[7], c->stream));
+                c->last_map_np = np;
+                c->last_map_nd = nd;
+                c->last_map_Lq = Lq;
+                c->last_map_p0 = s.p0;
+                c->last_map_pass_idx = mp.pass_idx;
+                c->last_map_pass_dst = mp.pass_dst;
                 CBP_CUDA(cudaMemcpyAsync(&c->h_maperr, c->maperr.p, sizeof(int), cudaMemcpyDeviceToHost,
                                          c->stream));
                 c->launches += 2;
@@ -1475,6 +1490,36 @@ int cbp_read_btck(cbp_context* c, uint8_t* btck, size_t ld)
         CBP_CUDA(cudaMemcpy2D(btck, ld, c->btck.as<uint8_t>() + c->last_row0 * c->last_ld, c->last_ld,
                               (size_t)c->last_ncols, c->last_Lq,
                               cudaMemcpyDeviceToHost));
+    });
+}
+
+int cbp_read_map_fb(cbp_context* c, size_t pair, float* fb, size_t ld, size_t* profile_len)
+{
+    return guarded([&] {
+        check_ctx(c);
+        if (!c->last_map_np) throw Error(CBP_ERR_STATE, "no MAP realignment in the last slab");
+        if (pair >= (size_t)c->last_map_np) throw Error(CBP_ERR_ARG, "pair index outside the last slab's pass list");
+        CBP_CUDA(cudaStreamSynchronize(c->stream));
+        int pidx = 0;
+        long long dst = 0;
+        CBP_CUDA(cudaMemcpy(&pidx, c->last_map_pass_idx + pair, sizeof(int), cudaMemcpyDeviceToHost));
+        CBP_CUDA(cudaMemcpy(&dst, c->last_map_pass_dst + pair, sizeof(long long), cudaMemcpyDeviceToHost));
+        const int Ld = c->db->h_plen[(size_t)(c->last_map_p0 + pidx)];
+        if (profile_len) *profile_len = (size_t)Ld;
+        if (!fb) return;
+        if (ld < (size_t)Ld) throw Error(CBP_ERR_ARG, "ld smaller than the profile length");
+        // the pair's diagonal rows [dst, dst + Ld + 31) of each 32-row band;
+        // cell (r, c) at local diagonal row c + r%32, lane r%32
+        const int Lq = c->last_map_Lq;
+        const size_t rows = (size_t)Ld + 31;
+        std::vector<float> band(rows * 32);
+        for (int b = 0; b * 32 < Lq; b++) {
+            const float* src = c->fb2.as<float>() + ((size_t)b * c->last_map_nd + (size_t)dst) * 32;
+            CBP_CUDA(cudaMemcpy(band.data(), src, band.size() * sizeof(float), cudaMemcpyDeviceToHost));
+            for (int t = 0; t < 32 && b * 32 + t < Lq; t++)
+                for (int col = 0; col < Ld; col++)
+                    fb[(size_t)(b * 32 + t) * ld + col] = band[((size_t)col + t) * 32 + t];
+        }
     });
 }
 

@@ -300,6 +300,17 @@ int cbp_read_btck(cbp_context* ctx, uint8_t* btck, size_t ld);
 int cbp_read_slab_columns(cbp_context* ctx, size_t first_col, size_t ncols, float* scores,
                           float* modscores, uint8_t* btck, size_t ld);
 
+/* The MAP stage's forward + backward log probabilities of the match state
+ * (the log of the posterior times Z) of pair `pair` of the last slab's pass
+ * list (record order within that slab), fb[r * ld + c] for the query rows r
+ * and the profile's columns c; *profile_len (may be NULL) receives the
+ * profile's length. Meaningful for the pairs the stage realigned (log
+ * E-value at most the threshold; MAPALN=1), of the last query processed.
+ * An inspection call with no counterpart in the reference, whose matrix is
+ * device-internal (src/libmycu/cumapdp/CuBatchMAPDP_bwd.cu); with fb ==
+ * NULL only the length is returned. CBP_ERR_STATE without a realignment. */
+int cbp_read_map_fb(cbp_context* ctx, size_t pair, float* fb, size_t ld, size_t* profile_len);
+
 /* Phase-1 score threshold and log E-value threshold from the E-value
  * threshold and the gapped Karlin-Altschul parameters (the [GAPPED_A_1]
  * lambda and K of cother.par); search space = query_len * db_len.

@@ -197,6 +197,11 @@ typedef struct orc_map_out {
 
 int orc_map_pair(const orc_map_in* in, orc_map_out* out);
 
+/* The same forward-backward in FP64 with exact exp/log: posterior of the
+ * match state of every cell, P[r*Ld + c], and log Z (an accuracy reference
+ * for the FP32 stage; not a restatement of the reference's arithmetic). */
+int orc_map_posteriors64(const orc_map_in* in, double* P, double* logz);
+
 /* MAPALN=0 (FinalizeDP_ALN, src/libmycu/cudp/CuBatchDP_aln_final.cu:40-430):
  * the alignment of the pair from its phase-1 backtrack codes btck1 ([Lq][ldb],
  * the pair's first column first), starting at the phase-1 maximum's

@@ -416,6 +416,47 @@ def map_pair(query, db, p, S, M, epa, minpp=0.28, modscores=True, printsss=True)
             "logz": mo.logz, "maxlogprob": mo.maxlogprob, "mapmax": mo.mapmax}
 
 
+def map_posteriors64(query, db, p, S, M, epa, modscores=True):
+    """The MAP forward-backward of query vs profile p in FP64 with exact
+    exp/log (orc_map_posteriors64): the match-state posterior of every cell
+    [Lq][Ld] (float64) and log Z. S, M as for map_pair."""
+    L = lib()
+    if not getattr(L, "_post64_bound", False):
+        L.orc_map_posteriors64.restype = ctypes.c_int
+        L.orc_map_posteriors64.argtypes = [ctypes.POINTER(MapIn), ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_double)]
+        L._post64_bound = True
+    p = int(p)
+    Lq = query.npositions
+    Ld = int(db.lens[p])
+    s0 = int(db.starts[p])
+    S = np.ascontiguousarray(S, np.float32)
+    M = np.ascontiguousarray(M, np.float32)
+    qtrn = np.ascontiguousarray(query.trn, np.float32)
+    dtrn = np.ascontiguousarray(db.trn, np.float32)
+    qaa = np.ascontiguousarray(query.aa, np.int8)
+    daa = np.ascontiguousarray(db.aa[s0:s0 + Ld], np.int8)
+    mi = MapIn(Lq, Ld, S.ctypes.data, M.ctypes.data, S.shape[1], qtrn.ctypes.data, qtrn.shape[1],
+               dtrn.ctypes.data + 4 * (s0 + p), dtrn.shape[1], float(epa), 0.28, int(modscores),
+               qaa.ctypes.data, daa.ctypes.data, qaa.ctypes.data, daa.ctypes.data, 0, 1, 1)
+    P = np.zeros((Lq, Ld), np.float64)
+    lz = ctypes.c_double()
+    L.orc_map_posteriors64(ctypes.byref(mi), P.ctypes.data, ctypes.byref(lz))
+    return P, lz.value
+
+
+def fast_expf(a):
+    """Schraudolph's exp as the MAP stage evaluates it (orc_fast_expf),
+    elementwise over a float32 array: the float32 fma 12102203.16*a +
+    1064631197 (exact in float64, then rounded once), truncated to int32 and
+    read as a float; 0 for a <= -16."""
+    a = np.asarray(a, np.float32)
+    t = (np.float64(np.float32(12102203.16)) * a.astype(np.float64)
+         + np.float64(np.float32(1064631197.0))).astype(np.float32)
+    out = np.trunc(t.astype(np.float64)).astype(np.int32).view(np.float32)
+    return np.where(np.float32(-16.0) < a, out, np.float32(0.0))
+
+
 def aln_pair(query, db, p, S, btck1, maxsc, maxr, maxc, printsss=True):
     """MAPALN=0: the alignment of query vs profile p from the phase-1
     backtrack codes btck1 ([Lq][Ld], the pair's columns) and the phase-1

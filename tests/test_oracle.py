@@ -131,3 +131,40 @@ def test_cvs_constants(oracle_lib):
     exact = (9.5 - 10.5) * (math.log(0.1) - math.log(2.1)) + sum(
         math.log(20 - i) - math.log(2) for i in range(1, 20))
     assert abs(ct - exact) < 1e-4
+
+
+def test_fast_expf_vectorized(oracle_lib):
+    """The vectorized Schraudolph exponential equals the oracle's C one bit
+    for bit (including its cut-off at -16)."""
+    import ctypes
+    L = oracle_lib.lib()
+    L.orc_fast_expf.restype = ctypes.c_float
+    L.orc_fast_expf.argtypes = [ctypes.c_float]
+    rng = np.random.default_rng(11)
+    a = np.concatenate([rng.uniform(-20.0, 4.0, 3000), rng.uniform(-1.0, 1.0, 1000),
+                        np.array([-16.0, -15.999999, 0.0, -0.0], np.float64)]).astype(np.float32)
+    got = oracle_lib.fast_expf(a)
+    ref = np.array([L.orc_fast_expf(float(x)) for x in a], np.float32)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+def test_map_posteriors_fp64_restatement(oracle_lib, ss_table):
+    """The FP64 forward-backward of the MAP stage: posteriors are
+    probabilities, the top-scoring cells of a planted homolog approach 1, and
+    the FP32 stage's posteriors (Schraudolph exp/log) lie within 0.25 of
+    them (the error the GPU test reports per form)."""
+    from cother_b200 import synth
+    O = oracle_lib
+    q = synth.make_profiles([90], 1201, True)
+    db = synth.make_profiles([120, 80], 1202, False)
+    synth.plant_homologs(q, db, 1.0, seed=1203)
+    sc, ms = O.score_matrix(q, db, ss_table, nthreads=4)
+    for p in range(db.nprofiles):
+        s0, Ld = int(db.starts[p]), int(db.lens[p])
+        S, M = sc[:, s0:s0 + Ld], ms[:, s0:s0 + Ld]
+        mo = O.map_pair(q, db, p, S, M, -30.0)
+        P64, lz = O.map_posteriors64(q, db, p, S, M, -30.0)
+        assert np.all(P64 >= 0.0) and np.all(P64 <= 1.0 + 1e-9)
+        assert P64.max() > 0.9 and np.isfinite(lz)
+        P32 = O.fast_expf(mo["fb"] - np.float32(mo["logz"])).astype(np.float64)
+        assert np.max(np.abs(P32 - P64)) < 0.25

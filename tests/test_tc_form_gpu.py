@@ -1,5 +1,6 @@
-"""The tensor-core forms of the profile-profile term (BF16x3 and TF32x3
-through cuBLAS) against the plain FP32 form and an FP64 restatement.
+"""The tensor-core forms of the profile-profile term (BF16x3 and TF32x3 on
+the tcgen05 tensor cores) against the plain FP32 form and an FP64
+restatement.
 
 With the SS and DDMS terms off, a cell's score is log(sum) - shift, where
 sum = sum_a q_a d_a / (0.5 (qbg_a + dbg_a)); the test computes the sums in
@@ -179,3 +180,64 @@ def test_fp64_parameter_fit(oracle_lib, ss_table):
     assert errs["lambda"] < 1e-4 and errs["K"] < 1e-3 and errs["H"] < 1e-4, errs
     print("\nFP32 parameter fit vs FP64 (%d pairs): max relative error lambda %.2e, K %.2e, H %.2e"
           % (nfit, errs["lambda"], errs["K"], errs["H"]))
+
+
+def test_map_posteriors_against_fp64(oracle_lib, ss_table):
+    """MAP posteriors of every form against FP64. For each pair the MAP
+    stage realigns (all terms on, planted homologs), the GPU's forward +
+    backward values equal the oracle's FP32 restatement of the stage bit for
+    bit, given the form's own cell scores. The posteriors the MAP DP reads,
+    exp(fb - log Z) with the stage's Schraudolph exponential, are compared
+    with the same model evaluated in FP64 with exact exp/log on the same
+    cells: the difference is the FP32 stage's, dominated by the fast
+    exp/log approximations that the reference uses and this build
+    reproduces. Also reported: each tensor-core form's posteriors against
+    the plain form's."""
+    import cother_b200 as cb
+    from cother_b200 import synth
+    O = oracle_lib
+    q = synth.make_profiles([150], 991, True)
+    db = synth.make_profiles(synth.lognormal_lengths(40, 150, 30, 400, seed=992), 993, False)
+    synth.plant_homologs(q, db, 0.2, seed=994)
+    Lq = q.npositions
+    report, post = {}, {}
+    for name, form in (("plain", cb.TC_PLAIN), ("bf16x3", cb.TC_BF16X3), ("tf32x3", cb.TC_TF32X3)):
+        o = cb.Options.defaults()
+        o.tc_form = form
+        with cb.BatchProcessing(ss_table, o) as bp:
+            bp.set_db_details(180 * 1000, 1000)
+            bp.transfer_cpm_data(db)
+            bp.process_score_matrix(q)
+            sc, ms, _ = bp.read_score_matrix(Lq, db.npositions)
+            recs = cb.records_table(bp.hit_records())
+            alns = bp.alignments(Lq)
+            st = cb.records_table(bp.read_statistics())
+            errs, n = [], 0
+            for k in range(len(recs["org_pro_no"])):
+                if alns[k] is None:
+                    continue
+                p = int(recs["org_pro_no"][k])
+                s0, Ld = int(db.starts[p]), int(db.lens[p])
+                S, M = sc[:, s0:s0 + Ld], ms[:, s0:s0 + Ld]
+                epa = float(st["log_evalue_pair"][k])
+                mo = O.map_pair(q, db, p, S, M, epa)
+                fb = bp.map_fb(k, Lq)
+                assert np.array_equal(fb.view(np.uint32), mo["fb"].view(np.uint32)), (name, p)
+                P32 = O.fast_expf(fb - np.float32(mo["logz"])).astype(np.float64)
+                P64, _ = O.map_posteriors64(q, db, p, S, M, epa)
+                big = P64 >= 0.01
+                errs.append((float(np.max(np.abs(P32 - P64))),
+                             float(np.max(np.abs(P32 - P64)[big] / P64[big])) if big.any() else 0.0))
+                post[(name, p)] = P32
+                n += 1
+        assert n >= 5, (name, n)
+        report[name] = (n, max(e[0] for e in errs), max(e[1] for e in errs))
+        assert report[name][1] < 0.25, (name, report[name])
+    vs_plain = {}
+    for name in ("bf16x3", "tf32x3"):
+        d = [float(np.max(np.abs(post[(name, p)] - post[("plain", p)])))
+             for (f, p) in post if f == "plain" and (name, p) in post]
+        vs_plain[name] = max(d) if d else float("nan")
+    print("\nform    pairs  posterior max-abs vs FP64  max rel (P64 >= 0.01)  max-abs vs plain")
+    for name, (n, a, r) in report.items():
+        print(f"{name:7s} {n:5d}  {a:24.3e}  {r:22.3e}  {vs_plain.get(name, 0.0):16.3e}")
