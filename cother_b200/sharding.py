@@ -16,7 +16,6 @@ positions (the work of the score matrix and the DPs grows with positions).
 """
 from __future__ import annotations
 
-import heapq
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -71,9 +70,11 @@ def local_hits(bp, first_profile: int, query_len: int):
 def merge_hit_lists(parts):
     """Stable merge of per-shard hit lists (each sorted by log E-value),
     shards in order: equal log E-values keep the shard order, then the
-    order within the shard."""
-    keyed = [[(h.log_evalue, k, i, h) for i, h in enumerate(part)] for k, part in enumerate(parts)]
-    return [t[3] for t in heapq.merge(*keyed, key=lambda t: (t[0], t[1], t[2]))]
+    order within the shard. The merge runs in the library's C++
+    (cbp_merge_hit_lists, the writer's join of a query's parts)."""
+    from .report import merge_hit_lists as merge_keys
+    keys = [np.array([h.log_evalue for h in part], np.float32) for part in parts]
+    return [parts[k][i] for k, i in merge_keys(keys)]
 
 
 def gather_hits(hits, group=None):
