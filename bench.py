@@ -532,8 +532,9 @@ def main():
                 "hbm_bytes_per_launch": float(Lq) * Ndb * 8,
                 "hbm_peak_gbs": (peaks or {}).get("hbm_gbs")}
         if args.ddmswgt <= 0:
-            # without DDMS the phase-1 DP dominates: its ALU roofline at 37
-            # algorithmic ops per cell (SURVEY's count for the 5-state DP)
+            # without DDMS the phase-1 DP weighs more: its ALU roofline at 37
+            # algorithmic ops per cell (23 adds, 9 maxima and 5 compares of
+            # the 5-state cell, CuBatchDP_init_btck.cu:303-360)
             dp_ms = stage_acc[1] / steps
             achieved = 37.0 * Lq * Ndb / (dp_ms / 1e3) / 1e9
             roof = {"bound": "alu", "achieved": achieved, "peak": alu_peak, "unit": "Gop/s",

@@ -1,4 +1,5 @@
-// Request loop over a resident database (the north star's serving form).
+// Request loop over a resident database: queries served as they arrive, with
+// continuous batching.
 //
 // The reference is a batch program: its job dispatcher hands whole queries
 // to per-GPU worker threads in round robin (src/libmycu/cualn/
