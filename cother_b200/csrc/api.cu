@@ -1262,6 +1262,7 @@ int cbp_transfer_chunk(cbp_context* c, char* const* beg, char* const* end, const
     return guarded([&] {
         check_ctx(c);
         c->have_db = false;
+        c->last_map_np = 0;   // the last search's phase-2 matrices refer to the old chunk
         // a fresh store: contexts sharing the previous one keep it
         auto st = std::make_shared<ProfilesStore>();
         upload_profiles(*st, beg, end, c->stream, c->opt.cvswgt > 0.0f);
@@ -1301,6 +1302,7 @@ int cbp_share_database(cbp_context* c, cbp_context* owner)
             throw Error(CBP_ERR_ARG, "contexts on different devices cannot share a database");
         if (!owner->have_db) throw Error(CBP_ERR_STATE, "the owner has no database chunk");
         CBP_CUDA(cudaStreamSynchronize(owner->stream));   // its upload has completed
+        c->last_map_np = 0;
         c->db = owner->db;
         c->have_db = true;
     });
