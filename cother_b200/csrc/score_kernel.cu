@@ -206,7 +206,13 @@ __device__ __forceinline__ float ddms_cell(const uint16_t* __restrict__ q, int l
     uint32_t me[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
     const float nsegm1 = -(float)(dstsegm - 1);
     float thr = kTiny;
-    if (dstsegm >= 5) {
+    if (dstsegm == 6) {
+        // the default DSTSEGM with its constant in the instructions (0.8 % faster)
+        for (int j = len2 >> 2; 0 <= j; j -= 2)
+            ddms_diagonal<true>(q, d + j, T, min(len1, len2 - j), 0, j, -5.0f, ms, mb, me, thr);
+        for (int i = len1 >> 2; 0 < i; i -= 2)
+            ddms_diagonal<true>(q + i, d, T, min(len2, len1 - i), i, 0, -5.0f, ms, mb, me, thr);
+    } else if (dstsegm >= 5) {
         for (int j = len2 >> 2; 0 <= j; j -= 2)
             ddms_diagonal<true>(q, d + j, T, min(len1, len2 - j), 0, j, nsegm1, ms, mb, me, thr);
         for (int i = len1 >> 2; 0 < i; i -= 2)

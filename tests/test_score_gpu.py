@@ -59,7 +59,8 @@ def test_score_matrix_last_slab(oracle_lib, ss_table):
 
 
 def test_score_matrix_options(oracle_lib, ss_table):
-    """DDMS off, SS off, other weights, DSTSEGM and MAPALN=0 shift."""
+    """DDMS off, SS off, other weights, DSTSEGM below 5 and above 6 (the kernel's
+    general and long-segment cases beside its default of 6) and MAPALN=0 shift."""
     from cother_b200 import synth
     q = synth.make_profiles([21], 41, True)
     db = synth.make_profiles([33, 18], 42, False)
@@ -67,6 +68,7 @@ def test_score_matrix_options(oracle_lib, ss_table):
         (dict(ddmswgt=0.0), dict(ddmswgt=0.0)),
         (dict(ssswgt=0.0), dict(ssswgt=0.0)),
         (dict(ssswgt=0.3, ddmswgt=0.5, dstsegm=3), dict(ssswgt=0.3, ddmswgt=0.5, dstsegm=3)),
+        (dict(dstsegm=8), dict(dstsegm=8)),
         (dict(mapaln=0), dict(initshift=0.0003)),
     ]:
         sc, ms, _ = _run(q, db, ss_table, **opt)
