@@ -557,7 +557,8 @@ def main():
                 "stage_ms": {k: v / steps for k, v in zip(STAGES, stage_acc)},
                 "gpu_launches": launches, "graph_launches": bp.graph_launches(),
                 "tuning": bp.tuning(Lq), "roofline": roof, "clocks": clocks}
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
+            # the host-core baseline: rank 0 of a one-GPU run only
             line["cpu_baseline"] = cpu_baseline(q, db, ss, args.cpu_seconds, db_len, nseqs, args.cvswgt)
     bp.close()
     if rank == 0:
