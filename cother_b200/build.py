@@ -49,6 +49,7 @@ CUDA_HEADERS = [
     "dp1_kernel.cuh",
     "tc_kernel.cuh",
     "hits_kernel.cuh",
+    "bulkcopy.cuh",
 ]
 
 

@@ -255,7 +255,7 @@ struct cbp_context {
     int last_map_p0 = 0;
     const int* last_map_pass_idx = nullptr;
     const long long* last_map_pass_dst = nullptr;
-    int h_dp1err = 0;   // set by the phase-1 DP when a staging wait gave up
+    int h_dp1err = 0;   // set when a staging wait gave up: 2 by the score kernel, 1 by the phase-1 DP
     bool score_thld_set = false, logE_thld_set = false;
     // results of the last process() call, all slabs
     std::vector<QueryResult> res;   // per query of the last call
@@ -797,6 +797,7 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
         a.dmstab = c->dmstab.as<float>();
         a.scores = c->scores.as<float>();
         a.modscores = c->modscores.as<float>();
+        a.err = c->dp1err.as<int>();   // shared with the phase-1 DP: 2 = score kernel, 1 = DP
         // the column order only balances the DDMS loops of a warp's lanes;
         // without that term the identity keeps the stores coalesced
         a.colorder = a.ddmswgt > 0.0f ? c->colorder.as<int>() : nullptr;
@@ -870,12 +871,12 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
                 else CBP_CUDA(cudaEventRecord(e, c->stream));
             };
             if (!tc) mark(c->ev[0]);
+            CBP_CUDA(cudaMemsetAsync(c->dp1err.p, 0, sizeof(int), c->stream));
             if (a.colorder)
                 launch_column_order(c->db->view.dstlen, s.col0, s.ncols, a.ld, tn.window, c->colorder.as<int>(),
                                     c->stream);
             launch_score_matrix(a, c->stream);
             mark(c->ev[1]);
-            CBP_CUDA(cudaMemsetAsync(c->dp1err.p, 0, sizeof(int), c->stream));
             dp_launches = 0;
             for (size_t k = 0; k < nq; k++) dp_launches += launch_dp1(d[k], c->stream);
             mark(c->ev[2]);
@@ -927,6 +928,8 @@ void process_queries(cbp_context* c, size_t nq, const size_t* qlens, char* const
             CBP_CUDA(cudaMemcpyAsync(&npass[k], pass_cnt(k), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         CBP_CUDA(cudaMemcpyAsync(&c->h_dp1err, c->dp1err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         CBP_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->h_dp1err == 2)
+            throw Error(CBP_ERR_CUDA, "score matrix: a wait for the bulk-copied distance lists timed out");
         if (c->h_dp1err)
             throw Error(CBP_ERR_CUDA, "phase-1 DP: a wait for staged score rows timed out");
         if (tc && c->h_tcerr)

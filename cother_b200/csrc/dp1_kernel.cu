@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "cbmath.cuh"
 #include "dp1_kernel.cuh"
+#include "bulkcopy.cuh"
 
 namespace cbp {
 
@@ -91,10 +92,6 @@ struct alignas(128) DpStage {
     unsigned long long bar[kSlots];    // completion of each slot's score rows
 };
 
-__device__ __forceinline__ unsigned smem_u32(const void* p)
-{
-    return (unsigned)__cvta_generic_to_shared(p);
-}
 __device__ __forceinline__ void cp_async4(void* dst, const float* src, bool valid)
 {
     const int n = valid ? 4 : 0;   // 0: fill with zeros, read nothing
@@ -104,45 +101,10 @@ __device__ __forceinline__ void cp_async4(void* dst, const float* src, bool vali
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* b)
+// a staging wait gives up after kWaitNs
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity)
 {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(b)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* b)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ bool mbar_test(unsigned long long* b, unsigned parity)
-{
-    unsigned ok;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(ok) : "r"(smem_u32(b)), "r"(parity) : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Wait for the phase of `parity` of an mbarrier to complete, for at most
-// kWaitNs; false if it did not.
-__device__ __noinline__ bool mbar_wait(unsigned long long* b, unsigned parity)
-{
-    if (mbar_test(b, parity)) return true;
-    const unsigned long long t0 = global_ns();
-    while (!mbar_test(b, parity))
-        if (global_ns() - t0 > kWaitNs) return false;
-    return true;
+    return mbar_wait_for(b, parity, kWaitNs);
 }
 
 // One cell of the 5-state DP (ExecDP_Btck_Unroll32x, CuBatchDP_init_btck.cu:
@@ -247,7 +209,7 @@ dp1_kernel(const Dp1Args a)
     if (kBulk) {
         if (lane == 0) {
             for (int j = 0; j < kSlots; j++) mbar_init(&st.bar[j]);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            mbar_init_fence();
         }
         __syncwarp();
     }

@@ -20,6 +20,7 @@
 #include "cbmath.cuh"
 #include "layout.h"
 #include "score_kernel.cuh"
+#include "bulkcopy.cuh"
 
 namespace cbp {
 
@@ -30,6 +31,9 @@ constexpr int kWarps = 4;
 constexpr int kThreads = kCols * kWarps;
 constexpr int kElems = 104;        // list elements held per position (99 + overrun)
 constexpr int kDbStride = 108;     // bytes per database list in shared memory (27 words)
+constexpr int kDbCopy = 112;       // bytes of a list brought in by one bulk copy (and its packed stride)
+constexpr int kDbWords = kDbStride / 4;
+constexpr unsigned long long kListWaitNs = 1000000000ull;   // the lists' copies: a wait gives up after 1 s
 
 // Top-3 register of non-intersecting segments
 // (src/libmycu/cusco/CuBatchScoreMatrix_ddms2s.cuh:182-251). The reference
@@ -270,7 +274,10 @@ score_matrix_kernel(const ScoreArgs a)
 {
     __shared__ float s_dms[kDstCard * kDstCard];
     __shared__ float s_sst[kSSCard * kSSCard];
-    __shared__ __align__(16) uint8_t s_dbe[kCols * kDbStride];
+    // the distance lists: first packed at kDbCopy bytes as the bulk copies
+    // leave them, then at the odd stride kDbStride with the codes times 4
+    __shared__ __align__(16) uint8_t s_dbe[kCols * kDbCopy];
+    __shared__ __align__(8) unsigned long long s_bar;
     __shared__ __align__(16) uint16_t s_qe[kRows * kElems];
     __shared__ float s_dtf[kNAA][kCols];
     __shared__ float s_dbg[kNAA][kCols];
@@ -300,9 +307,26 @@ score_matrix_kernel(const ScoreArgs a)
         const int slot = colb + tid;
         s_col[tid] = slot < a.ncols ? (a.colorder ? a.colorder[slot] : slot) : -1;
     }
-    for (int i = tid; a.ddmswgt > 0.0f && i < kDstCard * kDstCard; i += kThreads) s_dms[i] = a.dmstab[i] * 0x1p-7f;
+    const bool ddms = a.ddmswgt > 0.0f;
+    for (int i = tid; ddms && i < kDstCard * kDstCard; i += kThreads) s_dms[i] = a.dmstab[i] * 0x1p-7f;
     for (int i = tid; i < kSSCard * kSSCard; i += kThreads) s_sst[i] = a.sstab[i];
+    if (ddms && tid == 0) {
+        mbar_init(&s_bar);
+        mbar_init_fence();
+    }
     __syncthreads();
+
+    // the block's distance lists (DDMS only): one bulk copy per column,
+    // bytes 0..111 of its 128-byte list (this GPU's memory, 128-byte
+    // aligned) into s_dbe at a 112-byte stride, in flight while the
+    // column fields and the query rows below are read
+    if (ddms && warp == 0) {
+        const int cc = s_col[lane];
+        const unsigned ncopy = __popc(__ballot_sync(0xffffffffu, cc >= 0));
+        if (lane == 0) mbar_expect_tx(&s_bar, ncopy * (unsigned)kDbCopy);
+        __syncwarp();
+        if (cc >= 0) bulk_load(s_dbe + lane * kDbCopy, a.db.dst + (a.col0 + cc) * kDstStride, kDbCopy, &s_bar);
+    }
 
     // database columns of this block: lane l takes slab column s_col[l]
     const int col = s_col[lane];
@@ -322,24 +346,6 @@ score_matrix_kernel(const ScoreArgs a)
         if (warp == kNSS) s_dlen[lane] = a.db.dstlen[gpos];
     } else if (warp == kNSS) {
         s_dlen[lane] = 0;
-    }
-    // distance lists: 32 columns x 104 bytes, in 16-byte pieces, each code
-    // times 4 (a byte offset in a row of the pair-score table; codes <= 21,
-    // so the shift never carries across bytes); only for the DDMS term
-    const bool ddms = a.ddmswgt > 0.0f;
-    for (int idx = tid; ddms && idx < kCols * 7; idx += kThreads) {
-        const int c = idx / 7, piece = idx - c * 7;
-        const int cc = s_col[c];
-        uint4 v;
-        if (cc >= 0) {
-            v = *reinterpret_cast<const uint4*>(a.db.dst + (a.col0 + cc) * kDstStride + piece * 16);
-        } else {
-            const uint32_t f = 0x15151515u;  // kDstNoData in every byte
-            v = make_uint4(f, f, f, f);
-        }
-        uint32_t* dstw = reinterpret_cast<uint32_t*>(s_dbe + c * kDbStride + piece * 16);
-        dstw[0] = v.x << 2; dstw[1] = v.y << 2; dstw[2] = v.z << 2;
-        if (piece < 6) dstw[3] = v.w << 2;   // piece 6 covers bytes 96..107 only
     }
     // query rows of this block
     for (int idx = tid; idx < kRows * kNAA; idx += kThreads) {
@@ -383,6 +389,37 @@ score_matrix_kernel(const ScoreArgs a)
         o[1] = (uint16_t)(((v >> 8) & 0xffu) * (kDstCard * 4));
         o[2] = (uint16_t)(((v >> 16) & 0xffu) * (kDstCard * 4));
         o[3] = (uint16_t)((v >> 24) * (kDstCard * 4));
+    }
+    if (ddms) {
+        // the lists' copies: a wait that gives up flags the launch, waits
+        // once more for the copies still in flight into this block's
+        // shared memory, and ends the block without writing
+        const bool got = mbar_wait_for(&s_bar, 0, kListWaitNs);
+        if (__syncthreads_or(!got)) {
+            if (tid == 0 && a.err) atomicExch(a.err, 2);
+            (void)mbar_wait_for(&s_bar, 0, kListWaitNs);
+            return;
+        }
+        // to the odd stride, each code times 4 (a byte offset in a row of
+        // the pair-score table; codes <= 21, so the shift never carries
+        // across bytes); a slot without a column reads as no data
+        constexpr int kPer = (kCols * kDbWords + kThreads - 1) / kThreads;
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(s_dbe);
+        uint32_t w[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; k++) {
+            const int idx = tid + k * kThreads;
+            const int c = idx / kDbWords, wd = idx - c * kDbWords;
+            w[k] = 0x15151515u;   // kDstNoData in every byte
+            if (idx < kCols * kDbWords && s_col[c] >= 0) w[k] = src[c * (kDbCopy / 4) + wd];
+        }
+        __syncthreads();
+        uint32_t* dstw = reinterpret_cast<uint32_t*>(s_dbe);
+#pragma unroll
+        for (int k = 0; k < kPer; k++) {
+            const int idx = tid + k * kThreads;
+            if (idx < kCols * kDbWords) dstw[idx] = w[k] << 2;
+        }
     }
     __syncthreads();
 

@@ -35,6 +35,9 @@ struct ScoreArgs {
     // tensor-core form: the profile-profile sums, computed beforehand into
     // `scores` ([Lq][ld]), which the kernel then overwrites with the scores
     bool dots_in_scores = false;
+    // set to 2 when a wait for the bulk-copied distance lists gave up (may
+    // be null); the block then writes nothing
+    int* err = nullptr;
 };
 
 // columns per ordering window of launch_column_order: default and largest
