@@ -11,9 +11,11 @@
 //
 // DDMS dominates the cost (~550 segment-DP steps per cell for 99-distance
 // lists); it is CUDA-core ALU-bound, so the kernel is shaped for issue
-// efficiency: byte-packed distance lists in shared memory (odd word stride,
-// conflict-free for lanes in step), a 22x22 pair-score table in shared
-// memory, and one code path for upper and lower diagonals.
+// efficiency: byte-packed distance lists brought in by bulk copies and kept
+// in shared memory at an odd word stride (conflict-free for lanes in step),
+// a 22x22 pair-score table in shared memory, one code path for upper and
+// lower diagonals, and the step loop unrolled by four with DSTSEGM as
+// compile-time cases.
 #include <cmath>
 #include "cother_b200.h"
 #include "common.cuh"
